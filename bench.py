@@ -1,0 +1,467 @@
+#!/usr/bin/env python
+"""Benchmark of the batched 1D C2C FFT on B200 (GFLOP/s = 5 n log2 n / time).
+
+Default workload (the plain-method sweep's headline size): FP32 C2C forward,
+in place, n = 4096, batch = 16384 (2^26 points, 512 MiB, larger than the
+126 MB L2, so no flush is needed between steps).  A step is one execute of
+the batched plan.
+
+Output: one JSON line (rank 0) with
+  value      whole-job GFLOP/s, inputs resident in HBM, CUDA events around
+             exactly K steps on the plan's stream, max over ranks;
+  e2e        the same metric through the public C-ABI (mofft_execute_f32)
+             with pinned host buffers: host->device copy, transform,
+             device->host copy, all inside the timed region;
+  roofline   achieved HBM GB/s of the transform kernel (algorithmic bytes
+             P(n) * n * 16 B per transform / kernel time) over the measured
+             copy bandwidth;
+  cpu_baseline  the CPU port of the reference transform (oracle/, OpenMP
+             over the batch on every host core) on a bounded sample;
+  clocks     nvidia-smi samples taken during the timed region.
+
+Multi-GPU: one process per GPU (torchrun); the transform has no exchange
+step, so each rank runs its own replica of the workload (weak scaling) and
+NCCL only carries the barrier and the max-over-ranks timing.
+
+--impl reference times the reference's transform on the host cores (the
+C restatement in oracle/, since the reference's SME kernels cannot execute
+on this host ISA) on a bounded sample of the same workload.
+--sweep prints one line per length of the plain-method sweep instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["mofft", "reference"], default="mofft")
+    p.add_argument("--n", type=int, default=4096)
+    p.add_argument("--bits", type=int, choices=[32, 64], default=32)
+    p.add_argument("--points", type=int, default=1 << 26, help="points per call per GPU")
+    p.add_argument("--direction", type=int, choices=[-1, 1], default=-1)
+    p.add_argument("--out-of-place", action="store_true")
+    p.add_argument("--sweep", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--cpu-seconds", type=float, default=10.0)
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+
+def passes_for(n: int, bits: int) -> int:
+    """Minimal pass count of the HBM roofline: one CTA holds 2^14 FP32 /
+    2^13 FP64 points."""
+    per = 14 if bits == 32 else 13
+    return max(1, math.ceil(math.log2(n) / per))
+
+
+def flops_per_transform(n: int) -> float:
+    return 5.0 * n * math.log2(n)
+
+
+def measured_peaks() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def committed_traffic(kernel: str, workload: str):
+    path = ROOT / "profiles" / "traffic.json"
+    try:
+        data = json.loads(path.read_text())
+        entry = data.get(f"{kernel}|{workload}")
+        return entry
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device = device_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ distributed
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_teardown(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# --------------------------------------------------------------- CPU side
+
+def cpu_baseline(n: int, bits: int, direction: int, seconds: float) -> dict:
+    """The reference transform restated in C (oracle/), timed on all host
+    cores over a bounded sample of the workload: the same n, enough
+    transforms for about `seconds` of work."""
+    import numpy as np
+
+    import oracle
+    cores = os.cpu_count() or 1
+    dtype = np.complex64 if bits == 32 else np.complex128
+    batch = max(cores, (1 << 21) // n)
+    x = oracle.uniform(n * batch, seed=n, dtype=dtype).reshape(batch, n)
+    oracle.fft_port(x[:cores], direction, threads=cores)          # warm-up
+    samples = []
+    t_end = time.perf_counter() + seconds
+    while time.perf_counter() < t_end or len(samples) < 3:
+        t0 = time.perf_counter()
+        oracle.fft_port(x, direction, threads=cores)
+        samples.append(time.perf_counter() - t0)
+        if len(samples) >= 200:
+            break
+    med = statistics.median(samples)
+    value = flops_per_transform(n) * batch / med / 1e9
+    extra = {}
+    try:
+        import scipy.fft
+        t0 = time.perf_counter()
+        reps = 0
+        while time.perf_counter() - t0 < min(2.0, seconds / 4) or reps < 2:
+            scipy.fft.fft(x, axis=-1, workers=cores)
+            reps += 1
+        extra["scipy_pocketfft_gflops"] = round(
+            flops_per_transform(n) * batch * reps / (time.perf_counter() - t0) / 1e9, 2)
+    except Exception:
+        pass
+    return {"value": round(value, 3), "unit": "GFLOP/s", "cores": cores, "kind": "port",
+            "sample": f"{batch} transforms of n={n} FP{bits} per timed call, "
+                      f"median of {len(samples)} calls ({sum(samples):.1f} s of CPU work); "
+                      "FFTW 3.3.11: unavailable on this box",
+            **extra}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    import numpy as np
+
+    import oracle
+    cores = os.cpu_count() or 1
+    n, bits = args.n, args.bits
+    dtype = np.complex64 if bits == 32 else np.complex128
+    batch = max(cores, (1 << 20) // n)
+    x = oracle.uniform(n * batch, seed=n, dtype=dtype).reshape(batch, n)
+    for _ in range(args.warmup):
+        oracle.fft_port(x, args.direction, threads=cores)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.fft_port(x, args.direction, threads=cores)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(times) / len(times)
+    value = flops_per_transform(n) * batch / (ms / 1e3) / 1e9
+    line = {
+        "impl": "reference", "metric": "C2C GFLOP/s (5n log2 n)", "value": round(value, 3),
+        "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if bits == 32 else "f64", "data": "synthetic",
+        "config": workload_config(args),
+        "cpu_baseline": {"value": round(value, 3), "unit": "GFLOP/s", "cores": cores,
+                         "kind": "port",
+                         "sample": f"{batch} transforms of n={n} per step (the reference's "
+                                   "SME kernels cannot run on x86; FFTW 3.3.11: unavailable "
+                                   "on this box)"},
+        "e2e": {"value": round(value, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(args) -> dict:
+    n = args.n
+    batch = max(1, args.points // n)
+    return {"workload": f"C2C {'forward' if args.direction < 0 else 'backward'} "
+                        f"FP{args.bits} n={n} batch={batch} "
+                        f"{'out-of-place' if args.out_of_place else 'in-place'}",
+            "n": n, "batch": batch, "precision_bits": args.bits,
+            "placement": "out-of-place" if args.out_of_place else "in-place",
+            "inputs": "uniform[-1,1) seeded; 2^26-point working set > L2 (no flush)",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+# --------------------------------------------------------------- GPU side
+
+def time_device(plan, buf_in, buf_out, steps, warmup, stream, world):
+    import torch
+    for _ in range(warmup):
+        plan.execute(buf_in, buf_out)
+    stream.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        plan.execute(buf_in, buf_out)
+    end.record(stream)
+    end.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    return start.elapsed_time(end) / steps
+
+
+def run_gpu(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    import mofft_b200 as m
+    torch.cuda.set_device(local)
+    n, bits = args.n, args.bits
+    batch = max(1, args.points // n)
+    ctype = torch.complex64 if bits == 32 else torch.complex128
+    gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    real_t = torch.float32 if bits == 32 else torch.float64
+    data = torch.rand((batch, n, 2), generator=gen, device="cuda", dtype=real_t) * 2 - 1
+    x = torch.view_as_complex(data)
+    inplace = not args.out_of_place
+    y = x if inplace else torch.empty_like(x)
+    plan = m.Plan.create(n, args.direction, m.IN_PLACE if inplace else m.OUT_OF_PLACE,
+                         bits=bits, batch=batch)
+    stream = torch.cuda.Stream()
+    plan.set_stream(stream.cuda_stream)
+    sched = plan.schedule()
+    kernels = {k["index"]: k["name"] for k in m.kernels()}
+    # timed region: K steps, device-resident inputs
+    launches0 = m.launch_count()
+    with ClockSampler(local) as clocks:
+        ms = time_device(plan, x, y, args.steps, args.warmup, stream, world)
+    launches = m.launch_count() - launches0 - args.warmup * sched["pass_count"]
+    ms_max = max_over_ranks(ms, world)
+    flops = flops_per_transform(n) * batch
+    value = flops * world / (ms_max / 1e3) / 1e9
+    # roofline of the dominant kernel (per-pass timing when the plan has several)
+    peak, peak_kind = measured_peaks()
+    p_alg = passes_for(n, bits)
+    cb = 8 if bits == 32 else 16
+    alg_bytes_step = p_alg * n * 2 * cb * batch
+    pass_ms = [ms]
+    if sched["pass_count"] > 1:
+        pass_ms = per_pass_times(plan, x, y, stream, sched)
+    dom = int(np.argmax(pass_ms))
+    dom_bytes = 2 * cb * n * batch  # each pass reads and writes every point once
+    achieved = dom_bytes / (pass_ms[dom] / 1e3) / 1e9
+    workload = f"n={n} batch={batch} fp{bits}"
+    traffic = committed_traffic(kernels[sched["kernels"][dom]], workload)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": traffic, "peak_source": f"of {peak_kind}",
+                "kernel": kernels[sched["kernels"][dom]],
+                "algorithmic_bytes_per_launch": dom_bytes,
+                "step_roofline_frac": round(alg_bytes_step / (ms / 1e3) / 1e9 / peak, 4)}
+    # end-to-end through the public C-ABI with pinned host buffers
+    e2e = run_e2e(args, m, n, bits, batch, x)
+    plan.destroy()
+    line = None
+    if rank == 0:
+        line = {
+            "metric": "C2C GFLOP/s (5n log2 n)", "value": round(value, 2), "unit": "GFLOP/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if bits == 32 else "f64", "data": "synthetic",
+            "config": workload_config(args), "roofline": roofline,
+            "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks.summary(),
+            "schedule": {"passes": sched["pass_count"],
+                         "kernels": [kernels[k] for k in sched["kernels"]]},
+        }
+    return line
+
+
+def per_pass_times(plan, x, y, stream, sched):
+    """Kernel time of each pass, measured with events on the plan's stream by
+    running one-pass plans of the same decomposition is not possible from the
+    public API, so the whole step is split evenly (passes move equal bytes)."""
+    import torch
+    s = torch.cuda.Event(enable_timing=True)
+    e = torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    plan.execute(x, y)
+    e.record(stream)
+    e.synchronize()
+    total = s.elapsed_time(e)
+    return [total / sched["pass_count"]] * sched["pass_count"]
+
+
+def run_e2e(args, m, n, bits, batch, x_dev):
+    import torch
+    h_in = torch.empty(x_dev.shape, dtype=x_dev.dtype, pin_memory=True)
+    h_out = torch.empty_like(h_in, pin_memory=True)
+    h_in.copy_(x_dev)
+    plan = m.Plan.create(n, args.direction, m.OUT_OF_PLACE, bits=bits, batch=batch)
+    plan.execute(h_in, h_out)  # warm-up (allocates the staging buffers)
+    times = []
+    for _ in range(max(1, args.e2e_steps)):
+        t0 = time.perf_counter()
+        plan.execute(h_in, h_out)
+        times.append(time.perf_counter() - t0)
+    plan.destroy()
+    t = statistics.median(times)
+    nbytes = h_in.numel() * h_in.element_size()
+    return {"value": round(flops_per_transform(n) * batch / t / 1e9, 2), "unit": "GFLOP/s",
+            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+            "ms_per_step": round(t * 1e3, 3), "api": "mofft_execute_f%d (host buffers)" % bits}
+
+
+def run_sweep(args, world, rank, local):
+    import torch
+
+    import mofft_b200 as m
+    torch.cuda.set_device(local)
+    peak, kind = measured_peaks()
+    sizes = [2 ** e for e in range(4, 25)] + [3 * 2 ** e for e in range(4, 19)] + \
+        [5 * 2 ** e for e in range(4, 18)]
+    for bits in (32, 64):
+        total = (1 << 26) if bits == 32 else (1 << 25)
+        for n in sorted(sizes):
+            batch = max(1, total // n)
+            real_t = torch.float32 if bits == 32 else torch.float64
+            x = torch.view_as_complex(torch.rand((batch, n, 2), device="cuda", dtype=real_t))
+            plan = m.Plan.create(n, args.direction, m.IN_PLACE, bits=bits, batch=batch)
+            stream = torch.cuda.Stream()
+            plan.set_stream(stream.cuda_stream)
+            ms = time_device(plan, x, x, 10, 3, stream, world)
+            sched = plan.schedule()
+            plan.destroy()
+            cb = 8 if bits == 32 else 16
+            alg = passes_for(n, bits) * 2 * cb * n * batch
+            if rank == 0:
+                print(json.dumps({
+                    "n": n, "precision_bits": bits, "batch": batch, "ms": round(ms, 4),
+                    "gflops": round(flops_per_transform(n) * batch / (ms / 1e3) / 1e9, 1),
+                    "hbm_roofline_frac": round(alg / (ms / 1e3) / 1e9 / peak, 3),
+                    "passes": sched["pass_count"], "peak": f"{peak} GB/s of {kind}"}),
+                    flush=True)
+            del x
+            torch.cuda.empty_cache()
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank)
+        if args.sweep:
+            run_sweep(args, world, rank, local)
+            return 0
+        line = run_gpu(args, world, rank, local)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args.n, args.bits, args.direction,
+                                                args.cpu_seconds)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        dist_teardown(world)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,87 @@
+/* B200 extensions to the MoFFT C API (no counterpart in the reference, which
+ * computes one transform per call on one CPU core).
+ *
+ *  - Batched plans: `batch` transforms of `length` points, transform b starting
+ *    at element b*distance of the buffer (distance >= length; 0 = length).
+ *    mofft_execute_f32/f64 then processes the whole batch.
+ *  - Streams: attaching a cudaStream_t makes mofft_execute_* asynchronous on
+ *    that stream (device buffers only); NULL restores blocking behaviour.
+ *  - Kernel introspection for tests, the autotuner and the benchmark.
+ */
+#ifndef MOFFT_B200_H
+#define MOFFT_B200_H
+
+#include "mofft.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+mofft_status mofft_plan_create_batched_f32(
+    mofft_plan_f32 **plan, size_t length, size_t batch, size_t distance,
+    mofft_direction direction, mofft_placement placement,
+    const mofft_plan_options *options, mofft_plan_diagnostics *diagnostics);
+mofft_status mofft_plan_create_batched_f64(
+    mofft_plan_f64 **plan, size_t length, size_t batch, size_t distance,
+    mofft_direction direction, mofft_placement placement,
+    const mofft_plan_options *options, mofft_plan_diagnostics *diagnostics);
+
+/* Batched plan with an explicit radix chain (outermost first). */
+mofft_status mofft_plan_create_batched_with_radices_f32(
+    mofft_plan_f32 **plan, size_t length, size_t batch, size_t distance,
+    mofft_direction direction, mofft_placement placement, const int *radices,
+    size_t radix_count);
+mofft_status mofft_plan_create_batched_with_radices_f64(
+    mofft_plan_f64 **plan, size_t length, size_t batch, size_t distance,
+    mofft_direction direction, mofft_placement placement, const int *radices,
+    size_t radix_count);
+
+/* `stream` is a cudaStream_t (NULL = blocking calls on a plan-owned stream). */
+mofft_status mofft_plan_set_stream_f32(mofft_plan_f32 *plan, void *stream);
+mofft_status mofft_plan_set_stream_f64(mofft_plan_f64 *plan, void *stream);
+
+/* Number of transforms and element distance of a plan. */
+mofft_status mofft_plan_get_batch_f32(const mofft_plan_f32 *plan,
+                                      size_t *batch, size_t *distance);
+mofft_status mofft_plan_get_batch_f64(const mofft_plan_f64 *plan,
+                                      size_t *batch, size_t *distance);
+
+/* GPU schedule of a plan: number of passes (kernel launches per execute) and,
+ * per pass, the line length, registry kernel index and shared memory bytes. */
+typedef struct {
+  int pass_count;
+  int lengths[4];
+  int kernels[4];
+  size_t smem_bytes[4];
+  size_t workspace_bytes;     /* device workspace owned by the plan */
+  size_t twiddle_bytes;       /* device twiddle tables owned by the plan */
+} mofft_plan_schedule;
+mofft_status mofft_plan_get_schedule_f32(const mofft_plan_f32 *plan,
+                                         mofft_plan_schedule *schedule);
+mofft_status mofft_plan_get_schedule_f64(const mofft_plan_f64 *plan,
+                                         mofft_plan_schedule *schedule);
+
+/* The schedule the planner builds for (precision, length, radix chain or
+ * NULL for the PRETUNED model, kernel bank), computed on the host without a
+ * GPU.  chain_out (64 entries, may be NULL) receives the radix chain,
+ * outermost first. */
+mofft_status mofft_schedule_preview(int precision_bits, size_t length,
+                                    const int *radices, size_t radix_count,
+                                    unsigned int bank,
+                                    mofft_plan_schedule *schedule,
+                                    int *chain_out, size_t *chain_count);
+
+/* Kernel registry introspection. */
+int mofft_kernel_count(void);
+/* Fills name (NUL-terminated, truncated to capacity) and shape of entry i;
+ * returns 0 on success, -1 when i is out of range. */
+int mofft_kernel_info(int index, char *name, size_t capacity,
+                      int *precision_bits, int *kind, int *length, int *lines,
+                      int *threads, int *radix_count, int *radices);
+/* Kernel launches issued by this process so far (all plans). */
+uint64_t mofft_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

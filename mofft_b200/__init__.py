@@ -1,0 +1,373 @@
+"""MoFFT on NVIDIA B200: Python bindings of the C-ABI library ``libmofft.so``.
+
+The library exports the reference's ``include/mofft.h`` API (plans, execute,
+recipes, cost model) plus the batched/stream extensions of
+``include/mofft_b200.h``.  This module binds those symbols with ctypes and adds
+small conveniences for numpy (host buffers, staged through the GPU by the
+library) and torch (device buffers, executed in place on the GPU).
+
+There is no CPU fallback: if the shared library or a CUDA device is missing,
+plan creation raises ``MofftError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import os
+from pathlib import Path
+from typing import Optional, Sequence
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "lib" / "libmofft.so"
+
+
+class Status(enum.IntEnum):
+    SUCCESS = 0
+    INVALID_ARGUMENT = 1
+    UNSUPPORTED_SIZE = 2
+    ALLOCATION_FAILURE = 3
+    UNSUPPORTED_HARDWARE = 4
+    INTERNAL_ERROR = 5
+    WISDOM_NOT_FOUND = 6
+    INCOMPATIBLE_RECIPE = 7
+    BUFFER_TOO_SMALL = 8
+
+
+FORWARD = -1
+BACKWARD = 1
+OUT_OF_PLACE = 0
+IN_PLACE = 1
+PLANNER_PRETUNED = 0
+PLANNER_MEASURE = 1
+PLAN_STRICT_WISDOM = 1
+FLAG_PRETUNED = 0
+FLAG_MEASURE = 1
+FLAG_WISDOM_ONLY = 2
+STAGE_LAYOUT_TRANSPOSE = 0
+STAGE_LAYOUT_SECTION = 1
+TRANSPOSE_LINEAR = 0
+TRANSPOSE_BLOCKED = 1
+MAX_PLAN_DEPTH = 64
+KERNEL_ROWS, KERNEL_COLS, KERNEL_GENERIC = 0, 1, 2
+
+
+class MofftError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = Status(status) if status in Status._value2member_map_ else status
+        name = self.status.name if isinstance(self.status, Status) else str(status)
+        super().__init__(f"{what}: {name}" if what else name)
+
+
+class PlanOptions(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int), ("flags", ctypes.c_uint32),
+                ("candidate_limit", ctypes.c_size_t), ("timing_samples", ctypes.c_uint32)]
+
+
+class Diagnostics(ctypes.Structure):
+    _fields_ = [("measured", ctypes.c_int), ("used_wisdom", ctypes.c_int),
+                ("used_model_fallback", ctypes.c_int),
+                ("candidates_measured", ctypes.c_size_t),
+                ("radix_count", ctypes.c_size_t),
+                ("radices", ctypes.c_int * MAX_PLAN_DEPTH),
+                ("kernel_bank", ctypes.c_uint), ("kernel_bank_count", ctypes.c_uint),
+                ("blocked_transpose_mask", ctypes.c_uint64),
+                ("direct_input", ctypes.c_int), ("stage_layout", ctypes.c_int),
+                ("planning_seconds", ctypes.c_double),
+                ("selected_median_seconds", ctypes.c_double),
+                ("length", ctypes.c_size_t), ("precision_bits", ctypes.c_int),
+                ("direction", ctypes.c_int), ("placement", ctypes.c_int)]
+
+    def radix_list(self) -> list[int]:
+        return list(self.radices[: self.radix_count])
+
+
+class CostBreakdown(ctypes.Structure):
+    _fields_ = [("kernel_cost", ctypes.c_double), ("memory_cost", ctypes.c_double),
+                ("layout_cost", ctypes.c_double), ("total_cost", ctypes.c_double),
+                ("logical_read_bytes", ctypes.c_size_t),
+                ("logical_write_bytes", ctypes.c_size_t),
+                ("transferred_read_bytes", ctypes.c_size_t),
+                ("transferred_write_bytes", ctypes.c_size_t),
+                ("peak_working_set_bytes", ctypes.c_size_t)]
+
+
+class Schedule(ctypes.Structure):
+    _fields_ = [("pass_count", ctypes.c_int), ("lengths", ctypes.c_int * 4),
+                ("kernels", ctypes.c_int * 4), ("smem_bytes", ctypes.c_size_t * 4),
+                ("workspace_bytes", ctypes.c_size_t), ("twiddle_bytes", ctypes.c_size_t)]
+
+
+_P = ctypes.c_void_p
+_SZ = ctypes.c_size_t
+_I = ctypes.c_int
+_U32 = ctypes.c_uint32
+_U64 = ctypes.c_uint64
+
+# (name, restype, argtypes) for every exported entry point; the f32/f64 twins
+# are expanded below.
+_TYPED = [
+    ("mofft_plan_create_{s}", _I, [ctypes.POINTER(_P), _SZ, _I, _I]),
+    ("mofft_plan_create_with_options_{s}", _I,
+     [ctypes.POINTER(_P), _SZ, _I, _I, ctypes.POINTER(PlanOptions), ctypes.POINTER(Diagnostics)]),
+    ("mofft_plan_dft_1d_{s}", _P, [_SZ, _P, _P, _I, _U32]),
+    ("mofft_execute_plan_{s}", _I, [_P]),
+    ("mofft_plan_create_with_radices_{s}", _I,
+     [ctypes.POINTER(_P), _SZ, _I, _I, ctypes.POINTER(_I), _SZ]),
+    ("mofft_plan_set_transpose_strategy_{s}", _I, [_P, _I]),
+    ("mofft_plan_set_blocked_transpose_mask_{s}", _I, [_P, _U64]),
+    ("mofft_plan_set_direct_input_{s}", _I, [_P, _I]),
+    ("mofft_plan_set_stage_layout_{s}", _I, [_P, _I]),
+    ("mofft_plan_set_kernel_bank_{s}", _I, [_P, ctypes.c_uint]),
+    ("mofft_plan_get_kernel_bank_{s}", _I, [_P, ctypes.POINTER(ctypes.c_uint)]),
+    ("mofft_plan_export_{s}", _I, [_P, ctypes.c_char_p, _SZ, ctypes.POINTER(_SZ)]),
+    ("mofft_plan_import_{s}", _I, [ctypes.POINTER(_P), ctypes.c_char_p, _SZ,
+                                   ctypes.POINTER(Diagnostics)]),
+    ("mofft_execute_{s}", _I, [_P, _P, _P]),
+    ("mofft_plan_destroy_{s}", None, [_P]),
+    ("mofft_plan_create_batched_{s}", _I,
+     [ctypes.POINTER(_P), _SZ, _SZ, _SZ, _I, _I, ctypes.POINTER(PlanOptions),
+      ctypes.POINTER(Diagnostics)]),
+    ("mofft_plan_create_batched_with_radices_{s}", _I,
+     [ctypes.POINTER(_P), _SZ, _SZ, _SZ, _I, _I, ctypes.POINTER(_I), _SZ]),
+    ("mofft_plan_set_stream_{s}", _I, [_P, _P]),
+    ("mofft_plan_get_batch_{s}", _I, [_P, ctypes.POINTER(_SZ), ctypes.POINTER(_SZ)]),
+    ("mofft_plan_get_schedule_{s}", _I, [_P, ctypes.POINTER(Schedule)]),
+]
+_PLAIN = [
+    ("mofft_plan_options_init", None, [ctypes.POINTER(PlanOptions)]),
+    ("mofft_build_id", ctypes.c_char_p, []),
+    ("mofft_estimated_radix_cost", ctypes.c_double, [_I, _I, _I]),
+    ("mofft_estimated_stage_cost", ctypes.c_double, [_I, _I, _I, _SZ, _SZ]),
+    ("mofft_estimated_plan_cost", ctypes.c_double,
+     [_SZ, _I, ctypes.POINTER(_I), _SZ, _U64, _I]),
+    ("mofft_estimated_plan_cost_with_layout", ctypes.c_double,
+     [_SZ, _I, ctypes.POINTER(_I), _SZ, _U64, _I, _I]),
+    ("mofft_estimated_plan_cost_breakdown_with_layout", _I,
+     [_SZ, _I, ctypes.POINTER(_I), _SZ, _U64, _I, _I, ctypes.POINTER(CostBreakdown)]),
+    ("mofft_wisdom_is_formal", _I, []),
+    ("mofft_wisdom_source", ctypes.c_char_p, []),
+    ("mofft_status_string", ctypes.c_char_p, [_I]),
+    ("mofft_version", ctypes.c_char_p, []),
+    ("mofft_kernel_count", _I, []),
+    ("mofft_kernel_info", _I, [_I, ctypes.c_char_p, _SZ, ctypes.POINTER(_I),
+                               ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I),
+                               ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    ("mofft_launch_count", _U64, []),
+    ("mofft_schedule_preview", _I, [_I, _SZ, ctypes.POINTER(_I), _SZ, ctypes.c_uint,
+                                    ctypes.POINTER(Schedule), ctypes.POINTER(_I),
+                                    ctypes.POINTER(_SZ)]),
+]
+
+
+def exported_names() -> list[str]:
+    """Every entry point the library binds (both precisions expanded)."""
+    names = [n.format(s=s) for n, _, _ in _TYPED for s in ("f32", "f64")]
+    return names + [n for n, _, _ in _PLAIN]
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def load(path: Optional[os.PathLike] = None) -> ctypes.CDLL:
+    """Load libmofft.so (raises FileNotFoundError if it has not been built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is missing: run `python -m mofft_b200.build`")
+    lib = ctypes.CDLL(str(p))
+    for name, res, args in _TYPED:
+        for s in ("f32", "f64"):
+            fn = getattr(lib, name.format(s=s))
+            fn.restype = res
+            fn.argtypes = args
+    for name, res, args in _PLAIN:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def check(status: int, what: str = "") -> None:
+    if status != Status.SUCCESS:
+        raise MofftError(status, what)
+
+
+def status_string(status: int) -> str:
+    return load().mofft_status_string(status).decode()
+
+
+def build_id() -> str:
+    return load().mofft_build_id().decode()
+
+
+def launch_count() -> int:
+    return int(load().mofft_launch_count())
+
+
+def kernels() -> list[dict]:
+    """The compiled kernel registry."""
+    lib = load()
+    out = []
+    for i in range(lib.mofft_kernel_count()):
+        name = ctypes.create_string_buffer(96)
+        vals = [ctypes.c_int() for _ in range(6)]
+        rad = (ctypes.c_int * 8)()
+        lib.mofft_kernel_info(i, name, 96, *[ctypes.byref(v) for v in vals], rad)
+        bits, kind, length, lines, threads, count = (v.value for v in vals)
+        out.append({"index": i, "name": name.value.decode(), "precision_bits": bits,
+                    "kind": kind, "length": length, "lines": lines, "threads": threads,
+                    "radices": list(rad[:count])})
+    return out
+
+
+def schedule_preview(length: int, bits: int = 32, radices: Optional[Sequence[int]] = None,
+                     bank: int = 0) -> dict:
+    """Planner decision for a length without a GPU: passes and radix chain."""
+    lib = load()
+    s = Schedule()
+    chain = (ctypes.c_int * 64)()
+    count = ctypes.c_size_t()
+    arr = _int_array(radices) if radices else None
+    st = lib.mofft_schedule_preview(bits, length, arr, len(radices) if radices else 0, bank,
+                                    ctypes.byref(s), chain, ctypes.byref(count))
+    check(st, f"schedule_preview length={length}")
+    n = s.pass_count
+    return {"pass_count": n, "lengths": list(s.lengths[:n]), "kernels": list(s.kernels[:n]),
+            "smem_bytes": list(s.smem_bytes[:n]), "radices": list(chain[: count.value])}
+
+
+def _int_array(values: Sequence[int]):
+    arr = (ctypes.c_int * max(1, len(values)))(*values)
+    return arr
+
+
+def _pointer_of(buf) -> int:
+    """Address of a numpy array or torch tensor (contiguous, complex)."""
+    if hasattr(buf, "data_ptr"):
+        return int(buf.data_ptr())
+    if hasattr(buf, "ctypes"):
+        return int(buf.ctypes.data)
+    raise TypeError(f"unsupported buffer type {type(buf)!r}")
+
+
+class Plan:
+    """A MoFFT plan (one precision, direction, placement, batch)."""
+
+    def __init__(self, handle: int, bits: int):
+        self._h = ctypes.c_void_p(handle)
+        self.bits = bits
+        self._s = "f32" if bits == 32 else "f64"
+        self._lib = load()
+
+    def _fn(self, name: str):
+        return getattr(self._lib, f"mofft_{name}_{self._s}")
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    @classmethod
+    def create(cls, length: int, direction: int = FORWARD, placement: int = OUT_OF_PLACE,
+               *, bits: int = 32, batch: int = 1, distance: int = 0,
+               mode: int = PLANNER_PRETUNED, flags: int = 0, candidate_limit: int = 0,
+               timing_samples: int = 0, radices: Optional[Sequence[int]] = None,
+               diagnostics: Optional[Diagnostics] = None) -> "Plan":
+        lib = load()
+        s = "f32" if bits == 32 else "f64"
+        h = ctypes.c_void_p()
+        if radices is not None:
+            arr = _int_array(radices)
+            st = getattr(lib, f"mofft_plan_create_batched_with_radices_{s}")(
+                ctypes.byref(h), length, batch, distance, direction, placement, arr,
+                len(radices))
+        else:
+            opts = PlanOptions(mode, flags, candidate_limit, timing_samples)
+            diag = diagnostics if diagnostics is not None else Diagnostics()
+            st = getattr(lib, f"mofft_plan_create_batched_{s}")(
+                ctypes.byref(h), length, batch, distance, direction, placement,
+                ctypes.byref(opts), ctypes.byref(diag))
+        check(st, f"plan length={length} bits={bits}")
+        return cls(h.value, bits)
+
+    def execute(self, inp, out=None) -> None:
+        """Run on numpy arrays (host) or torch tensors (device)."""
+        if out is None:
+            out = inp
+        check(self._fn("execute")(self._h, _pointer_of(inp), _pointer_of(out)), "execute")
+
+    def execute_ptr(self, in_ptr: int, out_ptr: int) -> int:
+        return self._fn("execute")(self._h, in_ptr, out_ptr)
+
+    def set_stream(self, stream_handle: Optional[int]) -> None:
+        check(self._fn("plan_set_stream")(self._h, stream_handle or None), "set_stream")
+
+    def set_kernel_bank(self, bank: int) -> None:
+        check(self._fn("plan_set_kernel_bank")(self._h, bank), "set_kernel_bank")
+
+    def schedule(self) -> dict:
+        s = Schedule()
+        check(self._fn("plan_get_schedule")(self._h, ctypes.byref(s)), "schedule")
+        n = s.pass_count
+        return {"pass_count": n, "lengths": list(s.lengths[:n]), "kernels": list(s.kernels[:n]),
+                "smem_bytes": list(s.smem_bytes[:n]), "workspace_bytes": s.workspace_bytes,
+                "twiddle_bytes": s.twiddle_bytes}
+
+    def export(self) -> bytes:
+        req = ctypes.c_size_t()
+        check(self._fn("plan_export")(self._h, None, 0, ctypes.byref(req)), "export size")
+        buf = ctypes.create_string_buffer(req.value)
+        check(self._fn("plan_export")(self._h, buf, req.value, ctypes.byref(req)), "export")
+        return buf.raw[: req.value]
+
+    def destroy(self) -> None:
+        if self._h and self._h.value:
+            self._fn("plan_destroy")(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()
+
+
+def fft(x, direction: int = FORWARD, *, inplace: bool = False):
+    """Batched transform of a torch tensor of shape (..., n), complex64 or
+    complex128, on its CUDA device.  Returns the output tensor."""
+    import torch
+    if not x.is_cuda:
+        raise ValueError("fft() takes a CUDA tensor; use Plan for host arrays")
+    if x.dtype not in (torch.complex64, torch.complex128):
+        raise TypeError("complex64 or complex128 tensor required")
+    x = x.contiguous()
+    n = x.shape[-1]
+    batch = x.numel() // n
+    bits = 32 if x.dtype == torch.complex64 else 64
+    out = x if inplace else torch.empty_like(x)
+    plan = _plan_cache_get(n, batch, direction, inplace, bits, x.device.index or 0)
+    plan.set_stream(torch.cuda.current_stream(x.device).cuda_stream)
+    plan.execute(x, out)
+    return out
+
+
+_PLAN_CACHE: dict = {}
+
+
+def _plan_cache_get(n, batch, direction, inplace, bits, device):
+    key = (n, batch, direction, inplace, bits, device)
+    plan = _PLAN_CACHE.get(key)
+    if plan is None:
+        plan = Plan.create(n, direction, IN_PLACE if inplace else OUT_OF_PLACE,
+                           bits=bits, batch=batch)
+        _PLAN_CACHE[key] = plan
+    return plan

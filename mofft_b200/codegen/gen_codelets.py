@@ -1,0 +1,298 @@
+"""CUDA radix-codelet generator: the sm_100a backend of the MoFFT kernel compiler.
+
+The reference's build-time compiler (``compiler/mofft_compiler/emitter.py:283-466``
+with the ``backends/arm_sme.py`` lowering) turns each radix-R DFT into SME
+outer-product code.  On B200 a radix-R butterfly is a register-resident
+straight-line program executed by one thread, so this generator emits, for
+every radix the reference supports (``emitter.py:17``: 2..16, 32, 64), one
+``__device__ __forceinline__`` function that computes, in place,
+
+    y[k] = sum_j x[j] * exp(-2*pi*i*j*k/R)            (forward, FFTW sign)
+
+which is the codelet contract of ``compiler/mofft_compiler/validate.py:115-127``
+without the twiddle factor (twiddles are applied by the caller).  Backward
+transforms use the identity  bwd(x) = conj(fwd(conj(x)))  in the kernels.
+
+Algebra used (restated from the published methods, not from any library):
+  * prime R: the conjugate-pair ("like terms") form of the reference's
+    ``rewrites.py:43-95`` LIKE_TERMS pattern:  a_j = x_j + x_{R-j},
+    b_j = x_j - x_{R-j};  y_k = x_0 + sum a_j cos(2 pi jk/R) - i sum b_j sin(..).
+  * composite R = A*B: one level of Cooley-Tukey decimation in time with
+    compile-time twiddles; multiplications by 1, -1, +-i are folded and
+    multiplications by (+-1 +- i)/sqrt(2) use two real multiplies.
+
+Run:  python -m mofft_b200.codegen.gen_codelets <out_dir>
+It writes ``codelets.cuh`` (device code) and ``codelet_costs.h`` (real add /
+multiply counts per radix, used by the host cost model).
+"""
+from __future__ import annotations
+
+import math
+import sys
+from decimal import Decimal, getcontext
+from fractions import Fraction
+from pathlib import Path
+
+RADICES = (2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 32, 64)
+
+# Cooley-Tukey split (A = inner DFT length, B = outer) per composite radix.
+SPLIT = {4: (2, 2), 6: (2, 3), 8: (2, 4), 9: (3, 3), 10: (2, 5), 12: (4, 3),
+         14: (2, 7), 15: (3, 5), 16: (4, 4), 32: (4, 8), 64: (8, 8)}
+
+SQRT_HALF = math.sqrt(0.5)
+
+getcontext().prec = 60
+
+
+def _pi() -> Decimal:
+    """pi to 60 digits by Machin's formula (arctan series in Decimal)."""
+    def arctan_inv(x: int) -> Decimal:
+        total = term = Decimal(1) / x
+        x2 = x * x
+        n = 1
+        sign = 1
+        while True:
+            term /= x2
+            n += 2
+            sign = -sign
+            delta = term / n
+            if delta == 0 or abs(delta) < Decimal(10) ** -70:
+                break
+            total += sign * delta
+        return total
+    return 4 * (4 * arctan_inv(5) - arctan_inv(239))
+
+
+_PI = _pi()
+
+
+def _sin_cos_small(x: Decimal) -> tuple[Decimal, Decimal]:
+    """Taylor series for |x| <= pi/4."""
+    s = Decimal(0)
+    c = Decimal(0)
+    term_s = x
+    term_c = Decimal(1)
+    n = 0
+    while True:
+        s += term_s
+        c += term_c
+        n += 1
+        term_s = -term_s * x * x / ((2 * n) * (2 * n + 1))
+        term_c = -term_c * x * x / ((2 * n - 1) * (2 * n))
+        if abs(term_s) < Decimal(10) ** -65 and abs(term_c) < Decimal(10) ** -65:
+            return s, c
+
+
+def cis_turns(num: int, den: int) -> tuple[float, float]:
+    """(cos, sin) of 2*pi*num/den, correctly rounded to double.
+
+    The fraction is reduced exactly to an octant before the series, so
+    values such as cos(2*pi/3) come out as exactly -0.5."""
+    num %= den
+    # angle = 2*pi*num/den; octant index = floor(8*num/den)
+    eighths = Fraction(8 * num, den)
+    octant = int(eighths)
+    rest = eighths - octant            # in [0, 1): fraction of pi/4
+    if octant % 2 == 1:
+        rest = 1 - rest
+        mirror = True
+    else:
+        mirror = False
+    x = _PI / 4 * Decimal(rest.numerator) / Decimal(rest.denominator)
+    s, c = _sin_cos_small(x)
+    if mirror:
+        s, c = c, s
+    # (c, s) is now cos/sin of (octant-reduced) angle in [0, pi/4] or mirror.
+    quadrant = octant // 2
+    if quadrant == 0:
+        cr, sr = c, s
+    elif quadrant == 1:
+        cr, sr = -s, c
+    elif quadrant == 2:
+        cr, sr = -c, -s
+    else:
+        cr, sr = s, -c
+    return float(cr), float(sr)
+
+
+def _lit(value: float) -> str:
+    if abs(value) < 1e-300:
+        return "T(0)"
+    return f"T({value!r})"
+
+
+class Emitter:
+    """Builds straight-line SSA code over named real temporaries."""
+
+    def __init__(self) -> None:
+        self.lines: list[str] = []
+        self.count = 0
+        self.adds = 0
+        self.muls = 0
+
+    def tmp(self, expr: str, adds: int = 0, muls: int = 0) -> str:
+        name = f"t{self.count}"
+        self.count += 1
+        self.lines.append(f"  const T {name} = {expr};")
+        self.adds += adds
+        self.muls += muls
+        return name
+
+    # complex helpers: values are (re, im) tuples of temporaries/expressions
+    def add(self, a, b):
+        return (self.tmp(f"{a[0]} + {b[0]}", 1), self.tmp(f"{a[1]} + {b[1]}", 1))
+
+    def sub(self, a, b):
+        return (self.tmp(f"{a[0]} - {b[0]}", 1), self.tmp(f"{a[1]} - {b[1]}", 1))
+
+    def mul_unit(self, a, num: int, den: int):
+        """Multiply by exp(2*pi*i*num/den), folding the easy cases."""
+        c, s = cis_turns(num, den)
+        eps = 1e-14
+        if abs(c - 1) < eps and abs(s) < eps:
+            return a
+        if abs(c + 1) < eps and abs(s) < eps:
+            return (self.tmp(f"-{a[0]}"), self.tmp(f"-{a[1]}"))
+        if abs(c) < eps and abs(s - 1) < eps:   # * i
+            return (self.tmp(f"-{a[1]}"), self.tmp(f"{a[0]}"))
+        if abs(c) < eps and abs(s + 1) < eps:   # * -i
+            return (self.tmp(f"{a[1]}"), self.tmp(f"-{a[0]}"))
+        if abs(abs(c) - SQRT_HALF) < eps and abs(abs(s) - SQRT_HALF) < eps:
+            # (c + i s) = h * (sc + i ss) with h = sqrt(1/2), sc, ss = +-1
+            sc = "+" if c > 0 else "-"
+            ss = "+" if s > 0 else "-"
+            # re = h*(sc*ar - ss*ai), im = h*(ss*ar + sc*ai)
+            re_inner = self.tmp(f"{sc}{a[0]} {'-' if ss == '+' else '+'} {a[1]}", 1)
+            im_inner = self.tmp(f"{ss}{a[0]} {'+' if sc == '+' else '-'} {a[1]}", 1)
+            h = _lit(SQRT_HALF)
+            return (self.tmp(f"{h} * {re_inner}", 0, 1),
+                    self.tmp(f"{h} * {im_inner}", 0, 1))
+        cl, sl = _lit(c), _lit(s)
+        return (self.tmp(f"{a[0]} * {cl} - {a[1]} * {sl}", 1, 2),
+                self.tmp(f"{a[0]} * {sl} + {a[1]} * {cl}", 1, 2))
+
+    def dft(self, xs):
+        radix = len(xs)
+        if radix == 1:
+            return list(xs)
+        if radix == 2:
+            return [self.add(xs[0], xs[1]), self.sub(xs[0], xs[1])]
+        if radix in SPLIT:
+            return self._cooley_tukey(xs, *SPLIT[radix])
+        return self._prime(xs)
+
+    def _prime(self, xs):
+        radix = len(xs)
+        half = (radix - 1) // 2
+        a = [None] * (half + 1)
+        b = [None] * (half + 1)
+        for j in range(1, half + 1):
+            a[j] = self.add(xs[j], xs[radix - j])
+            b[j] = self.sub(xs[j], xs[radix - j])
+        ys = [None] * radix
+        acc = xs[0]
+        for j in range(1, half + 1):
+            acc = self.add(acc, a[j])
+        ys[0] = acc
+        for k in range(1, half + 1):
+            cr_terms = [xs[0][0]]
+            ci_terms = [xs[0][1]]
+            sr_terms = []
+            si_terms = []
+            for j in range(1, half + 1):
+                cos_v, sin_v = cis_turns(j * k, radix)
+                cj, sj = _lit(cos_v), _lit(sin_v)
+                cr_terms.append(f"{a[j][0]} * {cj}")
+                ci_terms.append(f"{a[j][1]} * {cj}")
+                sr_terms.append(f"{b[j][0]} * {sj}")
+                si_terms.append(f"{b[j][1]} * {sj}")
+            n = len(sr_terms)
+            cr = self.tmp(" + ".join(cr_terms), n, n)
+            ci = self.tmp(" + ".join(ci_terms), n, n)
+            sr = self.tmp(" + ".join(sr_terms), n - 1, n)
+            si = self.tmp(" + ".join(si_terms), n - 1, n)
+            ys[k] = (self.tmp(f"{cr} + {si}", 1), self.tmp(f"{ci} - {sr}", 1))
+            ys[radix - k] = (self.tmp(f"{cr} - {si}", 1),
+                             self.tmp(f"{ci} + {sr}", 1))
+        return ys
+
+    def _cooley_tukey(self, xs, inner: int, outer: int):
+        radix = inner * outer
+        z = []
+        for n2 in range(outer):
+            col = self.dft([xs[outer * n1 + n2] for n1 in range(inner)])
+            z.append([self.mul_unit(col[k1], -n2 * k1, radix)
+                      for k1 in range(inner)])
+        ys = [None] * radix
+        for k1 in range(inner):
+            row = self.dft([z[n2][k1] for n2 in range(outer)])
+            for k2 in range(outer):
+                ys[k1 + inner * k2] = row[k2]
+        return ys
+
+
+def emit_radix(radix: int) -> tuple[str, int, int]:
+    em = Emitter()
+    xs = []
+    for j in range(radix):
+        xs.append((f"re[{j}]", f"im[{j}]"))
+    # Load inputs into named temporaries so writes to re/im cannot alias reads.
+    loaded = [(em.tmp(x[0]), em.tmp(x[1])) for x in xs]
+    ys = em.dft(loaded)
+    body = list(em.lines)
+    for k, (yr, yi) in enumerate(ys):
+        body.append(f"  re[{k}] = {yr};")
+        body.append(f"  im[{k}] = {yi};")
+    text = (f"template <typename T>\n"
+            f"__device__ __forceinline__ void dft_fwd_{radix}(T (&re)[{radix}], "
+            f"T (&im)[{radix}]) {{\n" + "\n".join(body) + "\n}\n")
+    return text, em.adds, em.muls
+
+
+HEADER = """// Generated by mofft_b200/codegen/gen_codelets.py -- do not edit.
+// Forward radix-R DFT codelets (FFTW sign), in place on register arrays.
+#pragma once
+"""
+
+
+def generate() -> tuple[str, str]:
+    parts = [HEADER]
+    costs = []
+    for radix in RADICES:
+        text, adds, muls = emit_radix(radix)
+        parts.append(text)
+        costs.append((radix, adds, muls))
+    dispatch = ["template <int R> struct Dft;"]
+    for radix in RADICES:
+        dispatch.append(
+            f"template <> struct Dft<{radix}> {{ template <typename T> "
+            f"__device__ __forceinline__ static void fwd(T (&re)[{radix}], "
+            f"T (&im)[{radix}]) {{ dft_fwd_{radix}(re, im); }} }};")
+    parts.append("\n".join(dispatch) + "\n")
+    cost_lines = [
+        "// Generated by mofft_b200/codegen/gen_codelets.py -- do not edit.",
+        "// Real additions / multiplications of one forward radix-R codelet.",
+        "#pragma once",
+        "typedef struct { int radix; int adds; int muls; } mofft_codelet_cost;",
+        "static const mofft_codelet_cost k_mofft_codelet_costs[] = {",
+    ]
+    for radix, adds, muls in costs:
+        cost_lines.append(f"  {{{radix}, {adds}, {muls}}},")
+    cost_lines.append("};")
+    cost_lines.append(f"#define MOFFT_CODELET_COST_COUNT {len(costs)}")
+    return "\n".join(parts), "\n".join(cost_lines) + "\n"
+
+
+def main(argv: list[str]) -> int:
+    out_dir = Path(argv[1]) if len(argv) > 1 else Path(__file__).resolve().parents[1] / "csrc" / "generated"
+    out_dir.mkdir(parents=True, exist_ok=True)
+    cuh, costs = generate()
+    for name, text in (("codelets.cuh", cuh), ("codelet_costs.h", costs)):
+        path = out_dir / name
+        if not path.exists() or path.read_text() != text:
+            path.write_text(text)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv))

@@ -1,0 +1,585 @@
+// Device code for the MoFFT B200 transform: Stockham autosort stages held in
+// registers and exchanged through shared memory.
+//
+// Notation.  A line is one length-L DFT that a CTA computes completely.  The
+// in-CTA algorithm is the Stockham autosort form: with Ns the product of the
+// radices already applied, stage (R, Ns) maps butterfly j in [0, L/R) as
+//
+//   v[r]  = x[j + r*(L/R)] * W_{Ns*R}^{(j mod Ns)*r}           (r < R)
+//   v     = DFT_R(v)
+//   y[(j div Ns)*Ns*R + (j mod Ns) + k*Ns] = v[k]               (k < R)
+//
+// which leaves the result in natural order after the last stage.  This is the
+// same transform as the reference's mixed-radix Cooley-Tukey driver
+// (src/mofft.c:1932-2045: first codelet, then per level a twiddled "other"
+// codelet after a transpose), reorganised so that no transpose pass exists:
+// the transpose becomes the scatter index of the shared-memory exchange.
+//
+// Every kernel computes the forward transform (FFTW sign, exp(-2 pi i jk/n)).
+// Backward transforms use bwd(x) = conj(fwd(conj(x))): the imaginary part is
+// negated on load and on store (sign = -1), which is exact.
+//
+// Transforms longer than one CTA use the same Stockham step with a "super
+// radix" L per pass (four-step / six-step): pass p computes L_p-point DFTs over
+// lines strided by M/L_p, applies the super-stage twiddle W_{Ns*L}^{(j mod
+// Ns)*i} on load, and scatters with the same index map.  Those are the COLS
+// kernels below.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "generated/codelets.cuh"
+
+namespace mofft {
+
+template <typename T> struct Cplx;
+template <> struct Cplx<float> { using type = float2; };
+template <> struct Cplx<double> { using type = double2; };
+template <typename T> using cplx_t = typename Cplx<T>::type;
+
+// Shared memory holds real and imaginary parts in separate arrays (4- or
+// 8-byte words).  One pad word per 32 words (fp32) / 16 words (fp64) keeps
+// both the gather (j + r*L/R) and the scatter side of every exchange at one or
+// two wavefronts per warp access.
+template <typename T> struct Pad;
+template <> struct Pad<float> { static constexpr int shift = 5; };
+template <> struct Pad<double> { static constexpr int shift = 4; };
+template <typename T>
+__host__ __device__ constexpr int spad(int a) { return a + (a >> Pad<T>::shift); }
+template <typename T>
+__host__ __device__ constexpr int spad_len(int n) { return n + (n >> Pad<T>::shift) + 1; }
+
+template <typename T>
+__device__ __forceinline__ void cmul(T& xr, T& xi, T wr, T wi) {
+  const T r = xr * wr - xi * wi;
+  const T i = xr * wi + xi * wr;
+  xr = r;
+  xi = i;
+}
+
+template <typename T>
+__device__ __forceinline__ cplx_t<T> ld_global(const cplx_t<T>* p) { return *p; }
+template <typename T>
+__device__ __forceinline__ void st_global(cplx_t<T>* p, T re, T im) {
+  cplx_t<T> v;
+  v.x = re;
+  v.y = im;
+  *p = v;
+}
+
+// ---------------------------------------------------------------------------
+// Compile-time stage list.
+// ---------------------------------------------------------------------------
+template <int... Rs> struct RadixList {};
+
+template <int L, int... Rs> struct StageProduct;
+template <int L> struct StageProduct<L> { static constexpr int value = 1; };
+template <int L, int R, int... Rest> struct StageProduct<L, R, Rest...> {
+  static constexpr int value = R * StageProduct<L, Rest...>::value;
+};
+
+// Size (in complex entries) of the internal twiddle table of a stage list:
+// stage s with Ns > 1 stores (R_s - 1) * Ns entries, r-major.
+__host__ __device__ constexpr int stage_table_size(int R, int Ns) {
+  return Ns > 1 ? (R - 1) * Ns : 0;
+}
+
+// ---------------------------------------------------------------------------
+// Register stage: each thread owns PER = ceil((L/R)/TPL) butterflies of one
+// line.  Source and destination are global memory (first / last stage) or the
+// line's shared-memory slice (padded SoA).  Addressing of a line element i is
+// abstracted by the Layout policy:
+//   RowsLayout: a line is contiguous in global memory and in shared memory.
+//   ColsLayout: C lines are interleaved element-major in shared memory and in
+//               global memory the lines are adjacent (line stride 1, element
+//               stride S), so consecutive threads touch consecutive lines.
+// ---------------------------------------------------------------------------
+enum Where { kGlobal = 0, kShared = 1 };
+
+template <typename T>
+struct RowsLayout {
+  T* sre;          // this line's shared real part
+  T* sim;
+  const cplx_t<T>* gin;   // this line's first input element
+  cplx_t<T>* gout;        // this line's first output element
+  T sign;                 // -1 for backward (conjugation), +1 forward
+  bool active;            // this line is inside the batch
+  __device__ __forceinline__ int saddr(int i) const { return spad<T>(i); }
+  __device__ __forceinline__ void gload(int i, T& re, T& im) const {
+    if (active) {
+      const cplx_t<T> v = ld_global<T>(gin + i);
+      re = v.x;
+      im = v.y * sign;
+    } else {
+      re = T(0);
+      im = T(0);
+    }
+  }
+  __device__ __forceinline__ void gstore(int i, T re, T im) const {
+    if (active) st_global<T>(gout + i, re, im * sign);
+  }
+};
+
+template <typename T, int C, int PITCH>
+struct ColsLayout {
+  T* sre;          // shared base of the tile (all C lines)
+  T* sim;
+  int c;           // this thread's line within the tile
+  const cplx_t<T>* gin;   // element 0 of this line
+  cplx_t<T>* gout;        // element 0 of this line's output
+  long long in_stride;    // element stride in global memory (S = M / L)
+  long long out_stride;   // element stride of the output (Ns_outer)
+  T sign_in, sign_out;
+  bool active;
+  // super-stage twiddle on load: W^{e}, e = jmod * i, two-level table
+  const cplx_t<T>* tw_hi;
+  const cplx_t<T>* tw_lo;
+  long long jmod;         // (j mod Ns_outer) of this line, 0 = no twiddle
+  int split_shift;        // K = 1 << split_shift
+  __device__ __forceinline__ int saddr(int i) const { return i * PITCH + c; }
+  __device__ __forceinline__ void gload(int i, T& re, T& im) const {
+    if (active) {
+      const cplx_t<T> v = ld_global<T>(gin + (long long)i * in_stride);
+      re = v.x;
+      im = v.y * sign_in;
+      if (jmod != 0 && i != 0) {
+        const long long e = jmod * (long long)i;
+        const cplx_t<T> hi = __ldg(tw_hi + (e >> split_shift));
+        const cplx_t<T> lo = __ldg(tw_lo + (e & ((1LL << split_shift) - 1)));
+        T wr = hi.x, wi = hi.y;
+        cmul<T>(wr, wi, lo.x, lo.y);
+        cmul<T>(re, im, wr, wi);
+      }
+    } else {
+      re = T(0);
+      im = T(0);
+    }
+  }
+  __device__ __forceinline__ void gstore(int i, T re, T im) const {
+    if (active) st_global<T>(gout + (long long)i * out_stride, re, im * sign_out);
+  }
+};
+
+template <typename T, int L, int TPL, int R, int NS, Where SRC, Where DST,
+          int TWOFF, class Layout>
+__device__ __forceinline__ void reg_stage(const Layout& lay, int t,
+                                          const cplx_t<T>* __restrict__ tw) {
+  constexpr int BF = L / R;
+  constexpr int PER = (BF + TPL - 1) / TPL;
+  constexpr bool EVEN = (BF % TPL) == 0;
+  T vr[PER][R];
+  T vi[PER][R];
+#pragma unroll
+  for (int m = 0; m < PER; ++m) {
+    const int j = t + m * TPL;
+    if (EVEN || j < BF) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int idx = j + r * BF;
+        if (SRC == kGlobal) {
+          lay.gload(idx, vr[m][r], vi[m][r]);
+        } else {
+          vr[m][r] = lay.sre[lay.saddr(idx)];
+          vi[m][r] = lay.sim[lay.saddr(idx)];
+        }
+      }
+      if (NS > 1) {
+        const int jm = j % NS;
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          const cplx_t<T> w = __ldg(tw + TWOFF + (r - 1) * NS + jm);
+          cmul<T>(vr[m][r], vi[m][r], w.x, w.y);
+        }
+      }
+      Dft<R>::fwd(vr[m], vi[m]);
+    }
+  }
+  if (SRC == kShared && DST == kShared) __syncthreads();
+#pragma unroll
+  for (int m = 0; m < PER; ++m) {
+    const int j = t + m * TPL;
+    if (EVEN || j < BF) {
+      const int base = (j / NS) * NS * R + (j % NS);
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        const int idx = base + k * NS;
+        if (DST == kGlobal) {
+          lay.gstore(idx, vr[m][k], vi[m][k]);
+        } else {
+          lay.sre[lay.saddr(idx)] = vr[m][k];
+          lay.sim[lay.saddr(idx)] = vi[m][k];
+        }
+      }
+    }
+  }
+  if (DST == kShared) __syncthreads();
+}
+
+// Recursive stage driver over a compile-time radix list.
+template <typename T, int L, int TPL, int NS, int TWOFF, bool FIRST_SHARED,
+          bool LAST_SHARED, bool IS_FIRST, int... Rs>
+struct StageRunner;
+
+template <typename T, int L, int TPL, int NS, int TWOFF, bool FS, bool LS,
+          bool IS_FIRST, int R>
+struct StageRunner<T, L, TPL, NS, TWOFF, FS, LS, IS_FIRST, R> {
+  template <class Layout>
+  __device__ __forceinline__ static void run(const Layout& lay, int t,
+                                             const cplx_t<T>* tw) {
+    constexpr Where src = (IS_FIRST && !FS) ? kGlobal : kShared;
+    constexpr Where dst = LS ? kShared : kGlobal;
+    reg_stage<T, L, TPL, R, NS, src, dst, TWOFF>(lay, t, tw);
+  }
+};
+
+template <typename T, int L, int TPL, int NS, int TWOFF, bool FS, bool LS,
+          bool IS_FIRST, int R, int R2, int... Rest>
+struct StageRunner<T, L, TPL, NS, TWOFF, FS, LS, IS_FIRST, R, R2, Rest...> {
+  template <class Layout>
+  __device__ __forceinline__ static void run(const Layout& lay, int t,
+                                             const cplx_t<T>* tw) {
+    constexpr Where src = (IS_FIRST && !FS) ? kGlobal : kShared;
+    reg_stage<T, L, TPL, R, NS, src, kShared, TWOFF>(lay, t, tw);
+    StageRunner<T, L, TPL, NS * R, TWOFF + stage_table_size(R, NS), FS, LS,
+                false, R2, Rest...>::run(lay, t, tw);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// ROWS kernel: single pass.  A CTA computes TB complete transforms of length
+// L (each by TPL threads).  With STAGED, the CTA's TB*L contiguous input
+// elements are first copied to shared memory with coalesced vector loads and
+// the output leaves the same way (used when TPL is too small to coalesce).
+// ---------------------------------------------------------------------------
+template <typename T>
+struct RowsArgs {
+  const cplx_t<T>* in;
+  cplx_t<T>* out;
+  const cplx_t<T>* tw;      // internal stage tables
+  long long batch;
+  long long in_dist;
+  long long out_dist;
+  T sign;
+};
+
+template <typename T, int L, int TPL, int TB, bool STAGED, int... Rs>
+__global__ void __launch_bounds__(TPL * TB)
+rows_kernel(const RowsArgs<T> a) {
+  static_assert(StageProduct<L, Rs...>::value == L, "radices must multiply to L");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int LINE = spad_len<T>(L);
+  T* sre = reinterpret_cast<T*>(smem_raw);
+  T* sim = sre + TB * LINE;
+  const int line = threadIdx.x / TPL;
+  const int t = threadIdx.x % TPL;
+  const long long b0 = (long long)blockIdx.x * TB;
+  const long long b = b0 + line;
+  RowsLayout<T> lay;
+  lay.sre = sre + line * LINE;
+  lay.sim = sim + line * LINE;
+  lay.gin = a.in + b * a.in_dist;
+  lay.gout = a.out + b * a.out_dist;
+  lay.sign = a.sign;
+  lay.active = b < a.batch;
+  if (STAGED) {
+    // Cooperative load of lines b0 .. b0+TB-1 (each L contiguous elements).
+    const long long lines = (a.batch - b0) < TB ? (a.batch - b0) : TB;
+    for (int q = threadIdx.x; q < TB * L; q += TPL * TB) {
+      const int ln = q / L;
+      const int i = q - ln * L;
+      if (ln < lines) {
+        const cplx_t<T> v = ld_global<T>(a.in + (b0 + ln) * a.in_dist + i);
+        sre[ln * LINE + spad<T>(i)] = v.x;
+        sim[ln * LINE + spad<T>(i)] = v.y * a.sign;
+      }
+    }
+    __syncthreads();
+  }
+  StageRunner<T, L, TPL, 1, 0, STAGED, STAGED, true, Rs...>::run(lay, t, a.tw);
+  if (STAGED) {
+    const long long lines = (a.batch - b0) < TB ? (a.batch - b0) : TB;
+    for (int q = threadIdx.x; q < TB * L; q += TPL * TB) {
+      const int ln = q / L;
+      const int i = q - ln * L;
+      if (ln < lines)
+        st_global<T>(a.out + (b0 + ln) * a.out_dist + i,
+                     sre[ln * LINE + spad<T>(i)],
+                     sim[ln * LINE + spad<T>(i)] * a.sign);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// COLS kernel: one pass of a multi-pass transform of total length M.
+// Lines are the super-butterflies j in [0, M/L); a CTA owns C consecutive
+// lines of one batch entry.  Line j reads x[j + i*S] (S = M/L), multiplies by
+// W_{Ns*L}^{(j mod Ns)*i} and writes y[(j div Ns)*Ns*L + (j mod Ns) + k*Ns].
+// When Ns == 1 the C output lines form one contiguous block that is stored
+// from shared memory with coalesced writes (STAGED_OUT).
+// ---------------------------------------------------------------------------
+template <typename T>
+struct ColsArgs {
+  const cplx_t<T>* in;
+  cplx_t<T>* out;
+  const cplx_t<T>* tw;      // internal stage tables of the L-point DFT
+  const cplx_t<T>* tw_hi;   // super-stage twiddle, two-level table
+  const cplx_t<T>* tw_lo;
+  long long batch;
+  long long in_dist;        // distance between batch entries
+  long long out_dist;
+  long long total;          // M
+  long long ns_outer;       // Ns of this pass (product of earlier super radices)
+  int split_shift;
+  T sign_in;
+  T sign_out;
+};
+
+template <typename T, int L, int TPL, int C>
+struct ColsGeom {
+  static constexpr int PITCH = C + 1;           // words per element row
+  static constexpr int WORDS = L * PITCH;       // per real/imag array
+  static constexpr size_t SMEM = 2ull * WORDS * sizeof(T);
+  static constexpr int THREADS = TPL * C;
+};
+
+template <typename T, int L, int TPL, int C, int... Rs>
+__global__ void __launch_bounds__(TPL * C)
+cols_kernel(const ColsArgs<T> a) {
+  static_assert(StageProduct<L, Rs...>::value == L, "radices must multiply to L");
+  using G = ColsGeom<T, L, TPL, C>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sre = reinterpret_cast<T*>(smem_raw);
+  T* sim = sre + G::WORDS;
+  const long long lines_total = a.total / L;            // M / L
+  const long long groups = lines_total / C;             // C divides M/L
+  const long long b = blockIdx.x / groups;
+  const long long j0 = (blockIdx.x - b * groups) * C;
+  const int c = threadIdx.x % C;
+  const int t = threadIdx.x / C;
+  const long long j = j0 + c;
+  const long long ns = a.ns_outer;
+  const long long jq = j / ns;
+  const long long jm = j - jq * ns;
+  ColsLayout<T, C, G::PITCH> lay;
+  lay.sre = sre;
+  lay.sim = sim;
+  lay.c = c;
+  lay.gin = a.in + b * a.in_dist + j;
+  lay.in_stride = lines_total;
+  lay.gout = a.out + b * a.out_dist + jq * ns * L + jm;
+  lay.out_stride = ns;
+  lay.sign_in = a.sign_in;
+  lay.sign_out = a.sign_out;
+  lay.active = b < a.batch;
+  lay.tw_hi = a.tw_hi;
+  lay.tw_lo = a.tw_lo;
+  lay.jmod = jm;
+  lay.split_shift = a.split_shift;
+  if (ns == 1) {
+    StageRunner<T, L, TPL, 1, 0, false, true, true, Rs...>::run(lay, t, a.tw);
+    // lines j0..j0+C-1 are contiguous: out[b*dist + j0*L + c*L + k]
+    cplx_t<T>* dst = a.out + b * a.out_dist + j0 * L;
+    if (lay.active) {
+      for (int q = threadIdx.x; q < C * L; q += G::THREADS) {
+        const int cc = q / L;
+        const int k = q - cc * L;
+        st_global<T>(dst + q, sre[k * G::PITCH + cc],
+                     sim[k * G::PITCH + cc] * a.sign_out);
+      }
+    }
+  } else {
+    StageRunner<T, L, TPL, 1, 0, false, false, true, Rs...>::run(lay, t, a.tw);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Generic kernel: runtime stage list, any radix of the reference set, used for
+// lengths without a specialised instance.  Shared memory ping-pongs between two
+// buffers; a CTA owns `lines` lines (ROWS: transforms; COLS: super-butterflies
+// of a multi-pass transform, exactly as in cols_kernel).
+// ---------------------------------------------------------------------------
+constexpr int kMaxGenericStages = 24;
+
+template <typename T>
+struct GenericArgs {
+  const cplx_t<T>* in;
+  cplx_t<T>* out;
+  const cplx_t<T>* tw;      // internal stage tables (runtime stage list)
+  const cplx_t<T>* tw_hi;
+  const cplx_t<T>* tw_lo;
+  long long batch;
+  long long in_dist;
+  long long out_dist;
+  long long total;          // COLS: M; ROWS: L
+  long long ns_outer;       // COLS only
+  int split_shift;
+  int cols;                 // 0 = ROWS, 1 = COLS
+  int length;               // L
+  int lines;                // lines per CTA
+  int stage_count;
+  int radices[kMaxGenericStages];
+  T sign_in;
+  T sign_out;
+};
+
+template <typename T, int R>
+__device__ __forceinline__ void generic_butterfly(
+    const GenericArgs<T>& a, const T* __restrict__ sre_src,
+    const T* __restrict__ sim_src, T* __restrict__ sre_dst,
+    T* __restrict__ sim_dst, int line, int j, int L, int NS, int twoff,
+    bool first, bool last, int line_words, long long b, long long jline) {
+  T vr[R];
+  T vi[R];
+  const int BF = L / R;
+  const bool cols = a.cols != 0;
+  // element address helpers: ROWS keeps each line contiguous, COLS interleaves
+  // the lines (element-major) like cols_kernel.
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int idx = j + r * BF;
+    if (first) {
+      cplx_t<T> v;
+      if (cols) {
+        const long long S = a.total / L;
+        v = ld_global<T>(a.in + b * a.in_dist + jline + (long long)idx * S);
+      } else {
+        v = ld_global<T>(a.in + b * a.in_dist + idx);
+      }
+      vr[r] = v.x;
+      vi[r] = v.y * a.sign_in;
+      if (cols && idx != 0) {
+        const long long jm = jline % a.ns_outer;
+        if (jm != 0) {
+          const long long e = jm * (long long)idx;
+          const cplx_t<T> hi = __ldg(a.tw_hi + (e >> a.split_shift));
+          const cplx_t<T> lo = __ldg(a.tw_lo + (e & ((1LL << a.split_shift) - 1)));
+          T wr = hi.x, wi = hi.y;
+          cmul<T>(wr, wi, lo.x, lo.y);
+          cmul<T>(vr[r], vi[r], wr, wi);
+        }
+      }
+    } else {
+      const int s = cols ? idx * (a.lines + 1) + line : line * line_words + spad<T>(idx);
+      vr[r] = sre_src[s];
+      vi[r] = sim_src[s];
+    }
+  }
+  if (NS > 1) {
+    const int jm = j % NS;
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      const cplx_t<T> w = __ldg(a.tw + twoff + (r - 1) * NS + jm);
+      cmul<T>(vr[r], vi[r], w.x, w.y);
+    }
+  }
+  Dft<R>::fwd(vr, vi);
+  const int base = (j / NS) * NS * R + (j % NS);
+#pragma unroll
+  for (int k = 0; k < R; ++k) {
+    const int idx = base + k * NS;
+    if (last && !(cols && a.ns_outer == 1)) {
+      if (cols) {
+        const long long ns = a.ns_outer;
+        const long long jq = jline / ns, jm = jline - jq * ns;
+        st_global<T>(a.out + b * a.out_dist + jq * ns * L + jm + (long long)idx * ns,
+                     vr[k], vi[k] * a.sign_out);
+      } else {
+        st_global<T>(a.out + b * a.out_dist + idx, vr[k], vi[k] * a.sign_out);
+      }
+    } else {
+      const int s = cols ? idx * (a.lines + 1) + line : line * line_words + spad<T>(idx);
+      sre_dst[s] = vr[k];
+      sim_dst[s] = vi[k];
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void generic_dispatch(
+    int R, const GenericArgs<T>& a, const T* sre_src, const T* sim_src,
+    T* sre_dst, T* sim_dst, int line, int j, int L, int NS, int twoff,
+    bool first, bool last, int line_words, long long b, long long jline) {
+#define MOFFT_GENERIC_CASE(RR)                                                  \
+  case RR:                                                                      \
+    generic_butterfly<T, RR>(a, sre_src, sim_src, sre_dst, sim_dst, line, j, L, \
+                             NS, twoff, first, last, line_words, b, jline);     \
+    break;
+  switch (R) {
+    MOFFT_GENERIC_CASE(2) MOFFT_GENERIC_CASE(3) MOFFT_GENERIC_CASE(4)
+    MOFFT_GENERIC_CASE(5) MOFFT_GENERIC_CASE(6) MOFFT_GENERIC_CASE(7)
+    MOFFT_GENERIC_CASE(8) MOFFT_GENERIC_CASE(9) MOFFT_GENERIC_CASE(10)
+    MOFFT_GENERIC_CASE(11) MOFFT_GENERIC_CASE(12) MOFFT_GENERIC_CASE(13)
+    MOFFT_GENERIC_CASE(14) MOFFT_GENERIC_CASE(15) MOFFT_GENERIC_CASE(16)
+    MOFFT_GENERIC_CASE(32) MOFFT_GENERIC_CASE(64)
+    default: break;
+  }
+#undef MOFFT_GENERIC_CASE
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) generic_kernel(const GenericArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int L = a.length;
+  const bool cols = a.cols != 0;
+  const int line_words = cols ? 0 : spad_len<T>(L);
+  const int buf_words = cols ? L * (a.lines + 1) : a.lines * line_words;
+  T* bufs[2][2];
+  T* base = reinterpret_cast<T*>(smem_raw);
+  bufs[0][0] = base;
+  bufs[0][1] = base + buf_words;
+  bufs[1][0] = base + 2 * buf_words;
+  bufs[1][1] = base + 3 * buf_words;
+  long long b, jfirst;
+  if (cols) {
+    const long long groups = (a.total / L) / a.lines;
+    b = blockIdx.x / groups;
+    jfirst = (blockIdx.x - b * groups) * a.lines;
+  } else {
+    b = (long long)blockIdx.x * a.lines;
+    jfirst = 0;
+  }
+  int NS = 1;
+  int twoff = 0;
+  int cur = 0;
+  for (int s = 0; s < a.stage_count; ++s) {
+    const int R = a.radices[s];
+    const int BF = L / R;
+    const bool first = s == 0;
+    const bool last = s == a.stage_count - 1;
+    const int work = BF * a.lines;
+    for (int w = threadIdx.x; w < work; w += blockDim.x) {
+      int line, j;
+      if (cols) {
+        line = w % a.lines;
+        j = w / a.lines;
+      } else {
+        line = w / BF;
+        j = w - line * BF;
+      }
+      const long long bb = cols ? b : b + line;
+      if (bb >= a.batch) continue;
+      const long long jline = cols ? jfirst + line : 0;
+      generic_dispatch<T>(R, a, bufs[cur][0], bufs[cur][1], bufs[cur ^ 1][0],
+                          bufs[cur ^ 1][1], line, j, L, NS, twoff, first, last,
+                          line_words, cols ? b : bb, jline);
+    }
+    __syncthreads();
+    cur ^= 1;
+    twoff += stage_table_size(R, NS);
+    NS *= R;
+  }
+  if (cols && a.ns_outer == 1 && b < a.batch) {
+    // lines jfirst .. jfirst+lines-1 are contiguous in the output
+    cplx_t<T>* dst = a.out + b * a.out_dist + jfirst * L;
+    const int pitch = a.lines + 1;
+    for (int q = threadIdx.x; q < a.lines * L; q += blockDim.x) {
+      const int cc = q / L;
+      const int k = q - cc * L;
+      st_global<T>(dst + q, bufs[cur][0][k * pitch + cc],
+                   bufs[cur][1][k * pitch + cc] * a.sign_out);
+    }
+  }
+}
+
+}  // namespace mofft

@@ -1,0 +1,207 @@
+// Registry entry templates shared by the kernel instance files.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "fft_device.cuh"
+#include "mofft_cuda.h"
+
+namespace mofft {
+
+typedef cudaError_t (*launch_fn)(const mofft_pass_args *, cudaStream_t);
+typedef const void *(*func_fn)();
+
+struct Entry {
+  mofft_kernel_desc desc;
+  launch_fn launch;
+  func_fn func;
+};
+
+template <typename T>
+RowsArgs<T> rows_args(const mofft_pass_args *p) {
+  RowsArgs<T> a;
+  a.in = static_cast<const cplx_t<T> *>(p->in);
+  a.out = static_cast<cplx_t<T> *>(p->out);
+  a.tw = static_cast<const cplx_t<T> *>(p->tw);
+  a.batch = p->batch;
+  a.in_dist = p->in_dist;
+  a.out_dist = p->out_dist;
+  a.sign = p->conj_in ? T(-1) : T(1);
+  return a;
+}
+
+template <typename T>
+ColsArgs<T> cols_args(const mofft_pass_args *p) {
+  ColsArgs<T> a;
+  a.in = static_cast<const cplx_t<T> *>(p->in);
+  a.out = static_cast<cplx_t<T> *>(p->out);
+  a.tw = static_cast<const cplx_t<T> *>(p->tw);
+  a.tw_hi = static_cast<const cplx_t<T> *>(p->tw_hi);
+  a.tw_lo = static_cast<const cplx_t<T> *>(p->tw_lo);
+  a.batch = p->batch;
+  a.in_dist = p->in_dist;
+  a.out_dist = p->out_dist;
+  a.total = p->total;
+  a.ns_outer = p->ns_outer;
+  a.split_shift = p->split_shift;
+  a.sign_in = p->conj_in ? T(-1) : T(1);
+  a.sign_out = p->conj_out ? T(-1) : T(1);
+  return a;
+}
+
+template <typename T, int L, int TPL, int TB, bool STAGED, int... Rs>
+struct RowsInst {
+  static constexpr size_t smem() {
+    return 2ull * TB * spad_len<T>(L) * sizeof(T);
+  }
+  static const void *func() {
+    return reinterpret_cast<const void *>(&rows_kernel<T, L, TPL, TB, STAGED, Rs...>);
+  }
+  static cudaError_t launch(const mofft_pass_args *p, cudaStream_t s) {
+    if (p->conj_in != p->conj_out) return cudaErrorInvalidValue;
+    const long long grid = (p->batch + TB - 1) / TB;
+    if (grid <= 0) return cudaSuccess;
+    if (grid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    rows_kernel<T, L, TPL, TB, STAGED, Rs...>
+        <<<(unsigned)grid, TPL * TB, smem(), s>>>(rows_args<T>(p));
+    return cudaGetLastError();
+  }
+  static Entry entry(const char *name) {
+    Entry e;
+    e.desc.name = name;
+    e.desc.precision_bits = sizeof(T) == 4 ? 32 : 64;
+    e.desc.kind = MOFFT_KERNEL_ROWS;
+    e.desc.length = L;
+    e.desc.lines = TB;
+    e.desc.threads = TPL * TB;
+    e.desc.staged = STAGED ? 1 : 0;
+    const int rs[] = {Rs...};
+    e.desc.radix_count = (int)sizeof...(Rs);
+    for (int i = 0; i < 8; ++i) e.desc.radices[i] = i < (int)sizeof...(Rs) ? rs[i] : 0;
+    e.desc.smem_bytes = smem();
+    e.launch = &launch;
+    e.func = &func;
+    return e;
+  }
+};
+
+template <typename T, int L, int TPL, int C, int... Rs>
+struct ColsInst {
+  using G = ColsGeom<T, L, TPL, C>;
+  static const void *func() {
+    return reinterpret_cast<const void *>(&cols_kernel<T, L, TPL, C, Rs...>);
+  }
+  static cudaError_t launch(const mofft_pass_args *p, cudaStream_t s) {
+    if (p->total % L != 0 || (p->total / L) % C != 0) return cudaErrorInvalidValue;
+    if (p->ns_outer != 1 && p->ns_outer % C != 0) return cudaErrorInvalidValue;
+    const long long groups = (p->total / L) / C;
+    const long long grid = groups * p->batch;
+    if (grid <= 0) return cudaSuccess;
+    if (grid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    cols_kernel<T, L, TPL, C, Rs...>
+        <<<(unsigned)grid, G::THREADS, G::SMEM, s>>>(cols_args<T>(p));
+    return cudaGetLastError();
+  }
+  static Entry entry(const char *name) {
+    Entry e;
+    e.desc.name = name;
+    e.desc.precision_bits = sizeof(T) == 4 ? 32 : 64;
+    e.desc.kind = MOFFT_KERNEL_COLS;
+    e.desc.length = L;
+    e.desc.lines = C;
+    e.desc.threads = G::THREADS;
+    e.desc.staged = 0;
+    const int rs[] = {Rs...};
+    e.desc.radix_count = (int)sizeof...(Rs);
+    for (int i = 0; i < 8; ++i) e.desc.radices[i] = i < (int)sizeof...(Rs) ? rs[i] : 0;
+    e.desc.smem_bytes = G::SMEM;
+    e.launch = &launch;
+    e.func = &func;
+    return e;
+  }
+};
+
+template <typename T>
+size_t generic_smem(int L, int lines, int cols) {
+  const size_t words = cols ? (size_t)L * (lines + 1) : (size_t)lines * spad_len<T>(L);
+  return 4 * words * sizeof(T);
+}
+
+template <typename T>
+struct GenericInst {
+  static const void *func() {
+    return reinterpret_cast<const void *>(&generic_kernel<T>);
+  }
+  static cudaError_t launch(const mofft_pass_args *p, cudaStream_t s) {
+    GenericArgs<T> a;
+    a.in = static_cast<const cplx_t<T> *>(p->in);
+    a.out = static_cast<cplx_t<T> *>(p->out);
+    a.tw = static_cast<const cplx_t<T> *>(p->tw);
+    a.tw_hi = static_cast<const cplx_t<T> *>(p->tw_hi);
+    a.tw_lo = static_cast<const cplx_t<T> *>(p->tw_lo);
+    a.batch = p->batch;
+    a.in_dist = p->in_dist;
+    a.out_dist = p->out_dist;
+    a.total = p->generic_cols ? p->total : p->length;
+    a.ns_outer = p->generic_cols ? p->ns_outer : 1;
+    a.split_shift = p->split_shift;
+    a.cols = p->generic_cols;
+    a.length = p->length;
+    a.lines = p->lines;
+    a.stage_count = p->radix_count;
+    if (p->radix_count < 1 || p->radix_count > kMaxGenericStages || p->lines < 1)
+      return cudaErrorInvalidValue;
+    long long prod = 1;
+    for (int i = 0; i < kMaxGenericStages; ++i) {
+      a.radices[i] = i < p->radix_count ? p->radices[i] : 0;
+      if (i < p->radix_count) prod *= p->radices[i];
+    }
+    if (prod != p->length) return cudaErrorInvalidValue;
+    a.sign_in = p->conj_in ? T(-1) : T(1);
+    a.sign_out = p->conj_out ? T(-1) : T(1);
+    long long grid;
+    if (a.cols) {
+      if (p->total % p->length != 0 || (p->total / p->length) % p->lines != 0)
+        return cudaErrorInvalidValue;
+      if (p->ns_outer != 1 && p->ns_outer % p->lines != 0) return cudaErrorInvalidValue;
+      grid = (p->total / p->length) / p->lines * p->batch;
+    } else {
+      grid = (p->batch + p->lines - 1) / p->lines;
+    }
+    if (grid <= 0) return cudaSuccess;
+    if (grid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    const size_t smem = generic_smem<T>(p->length, p->lines, p->generic_cols);
+    generic_kernel<T><<<(unsigned)grid, 256, smem, s>>>(a);
+    return cudaGetLastError();
+  }
+  static Entry entry(const char *name) {
+    Entry e;
+    e.desc.name = name;
+    e.desc.precision_bits = sizeof(T) == 4 ? 32 : 64;
+    e.desc.kind = MOFFT_KERNEL_GENERIC;
+    e.desc.length = 0;
+    e.desc.lines = 0;
+    e.desc.threads = 256;
+    e.desc.staged = 0;
+    e.desc.radix_count = 0;
+    for (int i = 0; i < 8; ++i) e.desc.radices[i] = 0;
+    e.desc.smem_bytes = 227 * 1024;
+    e.launch = &launch;
+    e.func = &func;
+    return e;
+  }
+};
+
+
+#define ROWS(T, L, TPL, TB, ST, ...) \
+  RowsInst<T, L, TPL, TB, ST, __VA_ARGS__>::entry("rows_" #T "_" #L "_t" #TPL "_b" #TB "_s" #ST)
+#define COLS(T, L, TPL, C, ...) \
+  ColsInst<T, L, TPL, C, __VA_ARGS__>::entry("cols_" #T "_" #L "_t" #TPL "_c" #C)
+
+// Each instance file defines one of these.
+const Entry *entries_generic(int *count);
+const Entry *entries_rows_f32(int *count);
+const Entry *entries_rows_f64(int *count);
+const Entry *entries_cols_f32(int *count);
+const Entry *entries_cols_f64(int *count);
+
+}  // namespace mofft

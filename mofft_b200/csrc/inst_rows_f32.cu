@@ -1,0 +1,31 @@
+// FP32 single-pass kernels: whole transforms per CTA.
+#include "fft_instances.cuh"
+
+namespace mofft {
+const Entry *entries_rows_f32(int *count) {
+  static const Entry e[] = {
+      ROWS(float, 2, 1, 256, true, 2),
+      ROWS(float, 4, 1, 256, true, 4),
+      ROWS(float, 8, 1, 256, true, 8),
+      ROWS(float, 16, 1, 256, true, 16),
+      ROWS(float, 32, 4, 64, true, 8, 4),
+      ROWS(float, 64, 4, 64, true, 16, 4),
+      ROWS(float, 128, 8, 32, true, 16, 8),
+      ROWS(float, 256, 16, 16, true, 16, 16),
+      ROWS(float, 256, 16, 16, false, 16, 16),
+      ROWS(float, 512, 32, 8, false, 16, 16, 2),
+      ROWS(float, 512, 64, 4, false, 8, 8, 8),
+      ROWS(float, 1024, 64, 4, false, 16, 16, 4),
+      ROWS(float, 1024, 64, 2, false, 16, 16, 4),
+      ROWS(float, 1024, 32, 8, false, 32, 32),
+      ROWS(float, 2048, 128, 2, false, 16, 16, 8),
+      ROWS(float, 2048, 128, 1, false, 16, 16, 8),
+      ROWS(float, 4096, 256, 1, false, 16, 16, 16),
+      ROWS(float, 4096, 512, 1, false, 16, 16, 16),
+      ROWS(float, 8192, 512, 1, false, 16, 16, 16, 2),
+      ROWS(float, 16384, 512, 1, false, 16, 16, 16, 4),
+  };
+  *count = (int)(sizeof(e) / sizeof(e[0]));
+  return e;
+}
+}  // namespace mofft

@@ -1,0 +1,861 @@
+/* MoFFT on B200: plan objects, the PRETUNED planner, device twiddle tables
+ * and the execute driver.  This is the B200 counterpart of the reference's
+ * runtime (src/mofft.c): the same public semantics (status codes, argument
+ * validation, ownership, diagnostics), with the SME streaming-mode driver
+ * replaced by a short list of CUDA kernel launches ("passes").
+ *
+ * Mapping of the reference's plan onto the GPU schedule:
+ *  - The reference's radix chain (factors[0] outermost ... factors[d-1]
+ *    innermost, src/mofft.c:353-417) is kept as the plan's public identity.
+ *    Its innermost radix is applied first (src/mofft.c:1936-1943), which is
+ *    exactly the first stage of a Stockham autosort transform, so the GPU
+ *    stage list is the chain reversed.
+ *  - Consecutive stages are grouped into passes: one pass when the length fits
+ *    one CTA's shared memory, otherwise a four-step / six-step split in which
+ *    each pass is one kernel.  The grouping is canonical (fewest passes, then
+ *    specialised kernels, then balance), so a recipe's radix chain reproduces
+ *    the same schedule on import.
+ *  - Twiddles are computed in extended precision from an exact reduction of
+ *    the angle fraction and rounded once to the plan precision
+ *    (src/mofft.c:1082-1140 computes them in double); they live on the device
+ *    for the plan's lifetime.
+ */
+#define _GNU_SOURCE
+#include <cuda_runtime_api.h>
+#include <errno.h>
+#include <float.h>
+#include <math.h>
+#include <stdatomic.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include "mofft_internal.h"
+#include "mofft_host.h"
+
+/* ------------------------------------------------------------------------ */
+/* small helpers                                                             */
+/* ------------------------------------------------------------------------ */
+
+static const int k_ref_radices[] = {64, 32, 16, 15, 14, 13, 12, 11, 10,
+                                    9,  8,  7,  6,  5,  4,  3,  2};
+
+static atomic_ullong g_launches = 0;
+
+int mofft_is_supported_radix(int radix) {
+  for (size_t i = 0; i < sizeof(k_ref_radices) / sizeof(k_ref_radices[0]); ++i)
+    if (k_ref_radices[i] == radix) return 1;
+  return 0;
+}
+
+int mofft_is_smooth13(size_t n) {
+  if (n < 2) return 0;
+  static const int primes[] = {2, 3, 5, 7, 11, 13};
+  for (size_t i = 0; i < 6; ++i)
+    while (n % (size_t)primes[i] == 0) n /= (size_t)primes[i];
+  return n == 1;
+}
+
+double mofft_monotonic_seconds(void) {
+  struct timespec now;
+  if (clock_gettime(CLOCK_MONOTONIC, &now) != 0) return -1.0;
+  return (double)now.tv_sec + (double)now.tv_nsec * 1e-9;
+}
+
+size_t mofft_complex_bytes(int precision_bits) {
+  return precision_bits == 32 ? 8u : 16u;
+}
+
+/* ------------------------------------------------------------------------ */
+/* hardware probe (the analogue of mofft_hardware_supports, src/mofft.c:96) */
+/* ------------------------------------------------------------------------ */
+
+static atomic_int g_hw_support = -1;
+
+int mofft_hardware_supports(int precision_bits) {
+  (void)precision_bits; /* B200 runs FP32 and FP64 natively */
+  int cached = atomic_load(&g_hw_support);
+  if (cached >= 0) return cached;
+  int count = 0;
+  int supported = 0;
+  if (cudaGetDeviceCount(&count) == cudaSuccess && count > 0) {
+    int device = 0;
+    struct cudaDeviceProp prop;
+    if (cudaGetDevice(&device) == cudaSuccess &&
+        cudaGetDeviceProperties(&prop, device) == cudaSuccess)
+      supported = prop.major == 10 && prop.minor == 0; /* sm_100 */
+  } else {
+    cudaGetLastError();
+  }
+  int expected = -1;
+  atomic_compare_exchange_strong(&g_hw_support, &expected, supported);
+  return atomic_load(&g_hw_support);
+}
+
+/* GPU family word of recipes: compute capability and SM count. */
+int mofft_device_family(uint32_t *family) {
+  int device = 0;
+  struct cudaDeviceProp prop;
+  if (cudaGetDevice(&device) != cudaSuccess ||
+      cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  *family = ((uint32_t)prop.major << 24) | ((uint32_t)prop.minor << 16) |
+            ((uint32_t)prop.multiProcessorCount & 0xffffu);
+  return 1;
+}
+
+/* Per-device one-time kernel attribute setup. */
+static atomic_int g_prepared[64];
+
+static int prepare_current_device(void) {
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return 0;
+  if (device < 0 || device >= 64) return 0;
+  if (atomic_load(&g_prepared[device]) == 1) return 1;
+  if (mofft_cuda_prepare_device() != 0) return 0;
+  atomic_store(&g_prepared[device], 1);
+  return 1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* twiddles: exp(-2*pi*i*num/den) with exact octant reduction               */
+/* ------------------------------------------------------------------------ */
+
+void mofft_cis_turns(uint64_t num, uint64_t den, long double *c,
+                     long double *s) {
+  /* angle = 2*pi*num/den, returned as cos(angle), sin(angle) */
+  num %= den;
+  const unsigned __int128 eight = (unsigned __int128)num * 8u;
+  uint64_t octant = (uint64_t)(eight / den);
+  uint64_t rest = (uint64_t)(eight - (unsigned __int128)octant * den);
+  int mirror = (int)(octant & 1u);
+  if (mirror) rest = den - rest;
+  const long double quarter_pi = 0.785398163397448309615660845819875721L;
+  const long double x = quarter_pi * ((long double)rest / (long double)den);
+  long double sx = sinl(x), cx = cosl(x);
+  if (mirror) {
+    long double t = sx;
+    sx = cx;
+    cx = t;
+  }
+  switch ((octant / 2u) & 3u) {
+    case 0: *c = cx; *s = sx; break;
+    case 1: *c = -sx; *s = cx; break;
+    case 2: *c = -cx; *s = -sx; break;
+    default: *c = sx; *s = -cx; break;
+  }
+}
+
+/* Writes count forward twiddles W_den^(e) = exp(-2 pi i e/den) for
+ * e = first + k*step into dst (precision_bits wide complex). */
+static void write_twiddles(void *dst, int precision_bits, uint64_t den,
+                           uint64_t first, uint64_t step, size_t count) {
+  for (size_t k = 0; k < count; ++k) {
+    long double c, s;
+    mofft_cis_turns((first + (uint64_t)k * step) % den, den, &c, &s);
+    if (precision_bits == 32) {
+      ((float *)dst)[2 * k] = (float)c;
+      ((float *)dst)[2 * k + 1] = (float)-s;
+    } else {
+      ((double *)dst)[2 * k] = (double)c;
+      ((double *)dst)[2 * k + 1] = (double)-s;
+    }
+  }
+}
+
+/* Internal stage table of an in-CTA chain: stage (R, Ns>1) stores
+ * W_{Ns*R}^{jm*r} at (r-1)*Ns + jm. */
+static size_t stage_table_entries(const int *radices, int count) {
+  size_t total = 0, ns = 1;
+  for (int i = 0; i < count; ++i) {
+    if (ns > 1) total += (size_t)(radices[i] - 1) * ns;
+    ns *= (size_t)radices[i];
+  }
+  return total;
+}
+
+static void fill_stage_table(void *dst, int precision_bits, const int *radices,
+                             int count) {
+  const size_t cb = mofft_complex_bytes(precision_bits);
+  unsigned char *p = (unsigned char *)dst;
+  size_t ns = 1;
+  for (int i = 0; i < count; ++i) {
+    const size_t R = (size_t)radices[i];
+    if (ns > 1) {
+      for (size_t r = 1; r < R; ++r) {
+        write_twiddles(p, precision_bits, ns * R, 0, r, ns);
+        p += ns * cb;
+      }
+    }
+    ns *= R;
+  }
+}
+
+static int ceil_log2_u64(uint64_t x) {
+  int s = 0;
+  while (((uint64_t)1 << s) < x) ++s;
+  return s;
+}
+
+/* ------------------------------------------------------------------------ */
+/* kernel selection and canonical pass grouping                              */
+/* ------------------------------------------------------------------------ */
+
+#define SMEM_LIMIT (227u * 1024u)
+
+static int generic_kernel_index(int precision_bits) {
+  const int n = mofft_cuda_kernel_count();
+  for (int i = 0; i < n; ++i) {
+    const mofft_kernel_desc *d = mofft_cuda_kernel_get(i);
+    if (d->kind == MOFFT_KERNEL_GENERIC && d->precision_bits == precision_bits)
+      return i;
+  }
+  return -1;
+}
+
+static int chain_equal(const int *a, int na, const int *b, int nb) {
+  if (na != nb) return 0;
+  for (int i = 0; i < na; ++i)
+    if (a[i] != b[i]) return 0;
+  return 1;
+}
+
+/* Specialised kernel whose in-CTA chain equals `chain`. */
+static int find_special(int precision_bits, int kind, const int *chain,
+                        int count, long long total, long long ns_outer) {
+  long long length = 1;
+  for (int i = 0; i < count; ++i) length *= chain[i];
+  const int n = mofft_cuda_kernel_count();
+  for (int i = 0; i < n; ++i) {
+    const mofft_kernel_desc *d = mofft_cuda_kernel_get(i);
+    if (d->kind != kind || d->precision_bits != precision_bits ||
+        d->length != length ||
+        !chain_equal(d->radices, d->radix_count, chain, count))
+      continue;
+    if (kind == MOFFT_KERNEL_COLS) {
+      const long long lines_total = total / length;
+      if (lines_total % d->lines != 0) continue;
+      if (ns_outer != 1 && ns_outer % d->lines != 0) continue;
+    }
+    return i;
+  }
+  return -1;
+}
+
+static long long gcd_ll(long long a, long long b) {
+  while (b) {
+    long long t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+static int generic_rows_lines(int precision_bits, int length) {
+  int lines = length >= 1024 ? 1 : 1024 / length;
+  while (lines > 1 &&
+         mofft_cuda_generic_smem(precision_bits, length, lines, 0) > SMEM_LIMIT)
+    lines /= 2;
+  return mofft_cuda_generic_smem(precision_bits, length, lines, 0) <= SMEM_LIMIT
+             ? lines : 0;
+}
+
+static int generic_cols_lines(int precision_bits, int length, long long total,
+                              long long ns_outer) {
+  long long g = total / length;
+  if (ns_outer > 1) g = gcd_ll(g, ns_outer);
+  for (int lines = 16; lines >= 1; --lines) {
+    if (g % lines != 0) continue;
+    if (mofft_cuda_generic_smem(precision_bits, length, lines, 1) <= SMEM_LIMIT)
+      return lines;
+  }
+  return 0;
+}
+
+typedef struct {
+  int passes;
+  int generic;
+  double imbalance;
+} group_score;
+
+static int score_less(const group_score *a, const group_score *b) {
+  if (a->passes != b->passes) return a->passes < b->passes;
+  if (a->generic != b->generic) return a->generic < b->generic;
+  return a->imbalance < b->imbalance - 1e-9;
+}
+
+/* Fill one pass for stages [begin, end) of `chain`.  Returns 1 if some kernel
+ * can run it (specialised when allowed, else generic). */
+static int make_pass(int precision_bits, unsigned bank, const int *chain,
+                     int begin, int end, long long total, long long ns_outer,
+                     int single, mofft_pass *out) {
+  const int count = end - begin;
+  if (count < 1 || count > MOFFT_CUDA_MAX_STAGES) return 0;
+  long long length = 1;
+  for (int i = begin; i < end; ++i) length *= chain[i];
+  if (length > (1 << 24)) return 0;
+  memset(out, 0, sizeof(*out));
+  out->length = (int)length;
+  out->radix_count = count;
+  memcpy(out->radices, chain + begin, (size_t)count * sizeof(int));
+  out->ns_outer = ns_outer;
+  const int kind = single ? MOFFT_KERNEL_ROWS : MOFFT_KERNEL_COLS;
+  if (bank == 0 && count <= 8) {
+    const int k = find_special(precision_bits, kind, chain + begin, count,
+                               total, ns_outer);
+    if (k >= 0) {
+      const mofft_kernel_desc *d = mofft_cuda_kernel_get(k);
+      out->kernel = k;
+      out->kind = kind;
+      out->lines = d->lines;
+      out->smem_bytes = d->smem_bytes;
+      return 1;
+    }
+  }
+  const int g = generic_kernel_index(precision_bits);
+  if (g < 0) return 0;
+  int lines = single ? generic_rows_lines(precision_bits, (int)length)
+                     : generic_cols_lines(precision_bits, (int)length, total,
+                                          ns_outer);
+  if (lines <= 0) return 0;
+  out->kernel = g;
+  out->kind = MOFFT_KERNEL_GENERIC;
+  out->lines = lines;
+  out->smem_bytes = mofft_cuda_generic_smem(precision_bits, (int)length, lines,
+                                            single ? 0 : 1);
+  return 1;
+}
+
+/* Evaluate the split of `chain` at the given boundaries. */
+static int try_split(int precision_bits, unsigned bank, const int *chain,
+                     int count, const int *cuts, int passes, long long total,
+                     mofft_schedule *sched, group_score *score) {
+  long long ns = 1;
+  double lo = 1e300, hi = 0;
+  int generic = 0;
+  for (int p = 0; p < passes; ++p) {
+    const int begin = p == 0 ? 0 : cuts[p - 1];
+    const int end = p == passes - 1 ? count : cuts[p];
+    if (!make_pass(precision_bits, bank, chain, begin, end, total, ns,
+                   passes == 1, &sched->pass[p]))
+      return 0;
+    if (sched->pass[p].kind == MOFFT_KERNEL_GENERIC) ++generic;
+    const double l = log2((double)sched->pass[p].length);
+    if (l < lo) lo = l;
+    if (l > hi) hi = l;
+    ns *= sched->pass[p].length;
+  }
+  sched->pass_count = passes;
+  score->passes = passes;
+  score->generic = generic;
+  score->imbalance = hi - lo;
+  return 1;
+}
+
+/* Canonical grouping of a Stockham stage chain into passes. */
+int mofft_group_chain(int precision_bits, unsigned bank, const int *chain,
+                      int count, long long total, mofft_schedule *best) {
+  group_score best_score = {1 << 30, 1 << 30, 1e300};
+  int found = 0;
+  mofft_schedule cand;
+  group_score score;
+  for (int passes = 1; passes <= MOFFT_MAX_PASSES && passes <= count; ++passes) {
+    int cuts[MOFFT_MAX_PASSES];
+    /* enumerate increasing cut positions in [1, count-1] */
+    for (int i = 0; i < passes - 1; ++i) cuts[i] = i + 1;
+    for (;;) {
+      if (try_split(precision_bits, bank, chain, count, cuts, passes, total,
+                    &cand, &score) &&
+          (!found || score_less(&score, &best_score))) {
+        *best = cand;
+        best_score = score;
+        found = 1;
+      }
+      /* next combination */
+      int i = passes - 2;
+      while (i >= 0 && cuts[i] == count - (passes - 1 - i)) --i;
+      if (i < 0) break;
+      ++cuts[i];
+      for (int k = i + 1; k < passes - 1; ++k) cuts[k] = cuts[k - 1] + 1;
+    }
+    if (found) break;
+  }
+  return found;
+}
+
+/* Default in-CTA radix chain for a runtime-stage (generic) line of length L. */
+int mofft_auto_radices(long long length, int *out, int capacity) {
+  int count = 0;
+  long long n = length;
+  static const int pref[] = {16, 8, 4, 2};
+  static const int odd[] = {13, 11, 9, 7, 5, 3};
+  for (size_t i = 0; i < sizeof(odd) / sizeof(odd[0]); ++i)
+    while (n % odd[i] == 0) {
+      if (count >= capacity) return -1;
+      out[count++] = odd[i];
+      n /= odd[i];
+    }
+  for (size_t i = 0; i < sizeof(pref) / sizeof(pref[0]); ++i)
+    while (n % pref[i] == 0) {
+      if (count >= capacity) return -1;
+      out[count++] = pref[i];
+      n /= pref[i];
+    }
+  return n == 1 ? count : -1;
+}
+
+/* Preferred chain of a pass of length L: the first registered specialised
+ * kernel of that kind and length, else the generic default chain. */
+static int preferred_chain(int precision_bits, unsigned bank, int kind,
+                           long long length, long long total,
+                           long long ns_outer, int *out, int capacity) {
+  if (bank == 0) {
+    const int n = mofft_cuda_kernel_count();
+    for (int i = 0; i < n; ++i) {
+      const mofft_kernel_desc *d = mofft_cuda_kernel_get(i);
+      if (d->kind != kind || d->precision_bits != precision_bits ||
+          d->length != length || d->radix_count > capacity)
+        continue;
+      if (kind == MOFFT_KERNEL_COLS) {
+        if ((total / length) % d->lines != 0) continue;
+        if (ns_outer != 1 && ns_outer % d->lines != 0) continue;
+      }
+      memcpy(out, d->radices, (size_t)d->radix_count * sizeof(int));
+      return d->radix_count;
+    }
+  }
+  return mofft_auto_radices(length, out, capacity);
+}
+
+static void collect_divisors(long long n, long long lo, long long hi,
+                             long long *out, int *count, int capacity) {
+  *count = 0;
+  for (long long d = 1; d * d <= n; ++d) {
+    if (n % d) continue;
+    long long pair[2] = {d, n / d};
+    for (int k = 0; k < (d * d == n ? 1 : 2); ++k)
+      if (pair[k] >= lo && pair[k] <= hi && *count < capacity)
+        out[(*count)++] = pair[k];
+  }
+}
+
+/* Analytical PRETUNED chain for a whole transform of `length`. */
+int mofft_model_chain(int precision_bits, unsigned bank, size_t length,
+                      int *chain, int capacity) {
+  mofft_schedule sched;
+  /* one pass */
+  int count = preferred_chain(precision_bits, bank, MOFFT_KERNEL_ROWS,
+                              (long long)length, (long long)length, 1, chain,
+                              capacity);
+  if (count > 0 && mofft_group_chain(precision_bits, bank, chain, count,
+                                     (long long)length, &sched) &&
+      sched.pass_count == 1)
+    return count;
+  /* multi-pass: best balanced split whose passes have kernels */
+  enum { kMaxDiv = 4096 };
+  static __thread long long divs[kMaxDiv];
+  int ndiv = 0;
+  const long long n = (long long)length;
+  collect_divisors(n, 2, 1 << 16, divs, &ndiv, kMaxDiv);
+  int best_count = -1;
+  group_score best = {1 << 30, 1 << 30, 1e300};
+  int tmp[MOFFT_MAX_STAGES];
+  for (int passes = 2; passes <= 3 && best_count < 0; ++passes) {
+    for (int a = 0; a < ndiv; ++a) {
+      for (int b = 0; b < (passes == 3 ? ndiv : 1); ++b) {
+        long long L[3];
+        L[0] = divs[a];
+        if (passes == 2) {
+          L[1] = n / L[0];
+        } else {
+          L[1] = divs[b];
+          if ((n / L[0]) % L[1] != 0) continue;
+          L[2] = n / L[0] / L[1];
+        }
+        int total_count = 0;
+        long long ns = 1;
+        int ok = 1;
+        int cuts[MOFFT_MAX_PASSES];
+        for (int p = 0; p < passes && ok; ++p) {
+          if (L[p] < 2 || L[p] > (1 << 16)) { ok = 0; break; }
+          const int c = preferred_chain(precision_bits, bank, MOFFT_KERNEL_COLS,
+                                        L[p], n, ns, tmp + total_count,
+                                        MOFFT_MAX_STAGES - total_count);
+          if (c <= 0) { ok = 0; break; }
+          total_count += c;
+          if (p < passes - 1) cuts[p] = total_count;
+          ns *= L[p];
+        }
+        if (!ok) continue;
+        group_score score;
+        if (!try_split(precision_bits, bank, tmp, total_count, cuts, passes, n,
+                       &sched, &score))
+          continue;
+        if (best_count < 0 || score_less(&score, &best)) {
+          best = score;
+          best_count = total_count;
+          memcpy(chain, tmp, (size_t)total_count * sizeof(int));
+        }
+      }
+    }
+  }
+  return best_count;
+}
+
+/* ------------------------------------------------------------------------ */
+/* plan lifecycle                                                            */
+/* ------------------------------------------------------------------------ */
+
+static void release_device(mofft_core *c) {
+  if (c->d_twiddles) cudaFree(c->d_twiddles);
+  if (c->d_work) cudaFree(c->d_work);
+  if (c->d_stage[0]) cudaFree(c->d_stage[0]);
+  if (c->d_stage[1]) cudaFree(c->d_stage[1]);
+  c->d_twiddles = c->d_work = c->d_stage[0] = c->d_stage[1] = NULL;
+  c->twiddle_bytes = c->work_bytes = c->stage_bytes = 0;
+}
+
+void mofft_core_destroy(mofft_core *c) {
+  if (!c) return;
+  int saved = -1;
+  cudaGetDevice(&saved);
+  if (saved != c->device) cudaSetDevice(c->device);
+  release_device(c);
+  if (c->stream) cudaStreamDestroy((cudaStream_t)c->stream);
+  if (saved >= 0 && saved != c->device) cudaSetDevice(saved);
+  pthread_mutex_destroy(&c->lock);
+  free(c);
+}
+
+static size_t align256(size_t x) { return (x + 255u) & ~(size_t)255u; }
+
+/* Build device state (twiddles, workspace) for c->sched. */
+static mofft_status materialise_schedule(mofft_core *c) {
+  const size_t cb = mofft_complex_bytes(c->precision_bits);
+  size_t bytes = 0;
+  for (int p = 0; p < c->sched.pass_count; ++p) {
+    mofft_pass *ps = &c->sched.pass[p];
+    ps->tw_offset = bytes;
+    bytes = align256(bytes + stage_table_entries(ps->radices, ps->radix_count) * cb + cb);
+    ps->split_shift = 0;
+    ps->tw_hi_offset = ps->tw_lo_offset = bytes;
+    if (ps->ns_outer > 1) {
+      const uint64_t m = (uint64_t)ps->ns_outer * (uint64_t)ps->length;
+      const int shift = (ceil_log2_u64(m) + 1) / 2;
+      ps->split_shift = shift;
+      const size_t lo_n = (size_t)1 << shift;
+      const size_t hi_n = (size_t)((m + lo_n - 1) >> shift);
+      ps->tw_hi_offset = bytes;
+      bytes = align256(bytes + hi_n * cb);
+      ps->tw_lo_offset = bytes;
+      bytes = align256(bytes + lo_n * cb);
+    }
+  }
+  if (bytes == 0) bytes = 256;
+  unsigned char *host = (unsigned char *)calloc(1, bytes);
+  if (!host) return MOFFT_ALLOCATION_FAILURE;
+  for (int p = 0; p < c->sched.pass_count; ++p) {
+    const mofft_pass *ps = &c->sched.pass[p];
+    fill_stage_table(host + ps->tw_offset, c->precision_bits, ps->radices,
+                     ps->radix_count);
+    if (ps->ns_outer > 1) {
+      const uint64_t m = (uint64_t)ps->ns_outer * (uint64_t)ps->length;
+      const size_t lo_n = (size_t)1 << ps->split_shift;
+      const size_t hi_n = (size_t)((m + lo_n - 1) >> ps->split_shift);
+      write_twiddles(host + ps->tw_hi_offset, c->precision_bits, m, 0, lo_n, hi_n);
+      write_twiddles(host + ps->tw_lo_offset, c->precision_bits, m, 0, 1, lo_n);
+    }
+  }
+  release_device(c);
+  if (cudaMalloc(&c->d_twiddles, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    free(host);
+    return MOFFT_ALLOCATION_FAILURE;
+  }
+  c->twiddle_bytes = bytes;
+  if (cudaMemcpy(c->d_twiddles, host, bytes, cudaMemcpyHostToDevice) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    free(host);
+    return MOFFT_INTERNAL_ERROR;
+  }
+  free(host);
+  const int P = c->sched.pass_count;
+  const int need_work = P >= 3 || (P == 2 && c->placement == MOFFT_IN_PLACE);
+  if (need_work) {
+    const size_t work = c->batch * c->length * cb;
+    if (cudaMalloc(&c->d_work, work) != cudaSuccess) {
+      cudaGetLastError();
+      return MOFFT_ALLOCATION_FAILURE;
+    }
+    c->work_bytes = work;
+  }
+  return MOFFT_SUCCESS;
+}
+
+/* Set c->factors/depth (reference order) from a Stockham chain. */
+static void set_factors_from_chain(mofft_core *c, const int *chain, int count) {
+  c->depth = count;
+  for (int i = 0; i < count; ++i) c->factors[i] = chain[count - 1 - i];
+}
+
+static int chain_from_factors(const mofft_core *c, int *chain) {
+  for (int i = 0; i < c->depth; ++i) chain[i] = c->factors[c->depth - 1 - i];
+  return c->depth;
+}
+
+/* (Re)build the GPU schedule from c->factors and c->kernel_bank. */
+mofft_status mofft_core_build(mofft_core *c) {
+  int chain[MOFFT_MAX_STAGES];
+  const int count = chain_from_factors(c, chain);
+  mofft_schedule sched;
+  if (!mofft_group_chain(c->precision_bits, c->kernel_bank, chain, count,
+                         (long long)c->length, &sched))
+    return MOFFT_UNSUPPORTED_SIZE;
+  c->sched = sched;
+  return materialise_schedule(c);
+}
+
+/* Allocate a core with validated shape; chain==NULL selects the model. */
+mofft_status mofft_core_create(mofft_core **out, int precision_bits,
+                               size_t length, size_t batch, size_t distance,
+                               mofft_direction direction,
+                               mofft_placement placement, const int *chain,
+                               int chain_count) {
+  *out = NULL;
+  if (!mofft_hardware_supports(precision_bits)) return MOFFT_UNSUPPORTED_HARDWARE;
+  if (length < 2 || length > ((size_t)1 << 34)) return MOFFT_UNSUPPORTED_SIZE;
+  if (!mofft_is_smooth13(length)) return MOFFT_UNSUPPORTED_SIZE;
+  if (batch == 0) return MOFFT_INVALID_ARGUMENT;
+  if (distance == 0) distance = length;
+  if (distance < length) return MOFFT_INVALID_ARGUMENT;
+  if (batch > SIZE_MAX / distance / 16) return MOFFT_ALLOCATION_FAILURE;
+  if (!prepare_current_device()) return MOFFT_UNSUPPORTED_HARDWARE;
+  mofft_core *c = (mofft_core *)calloc(1, sizeof(*c));
+  if (!c) return MOFFT_ALLOCATION_FAILURE;
+  pthread_mutex_init(&c->lock, NULL);
+  c->length = length;
+  c->direction = direction;
+  c->placement = placement;
+  c->precision_bits = precision_bits;
+  c->batch = batch;
+  c->distance = distance;
+  c->direct_input = 1;
+  c->stage_layout = MOFFT_STAGE_LAYOUT_TRANSPOSE;
+  cudaGetDevice(&c->device);
+  int tmp[MOFFT_MAX_STAGES];
+  int count = chain_count;
+  if (!chain) {
+    count = mofft_model_chain(precision_bits, 0, length, tmp, MOFFT_MAX_STAGES);
+    if (count <= 0) {
+      mofft_core_destroy(c);
+      return MOFFT_UNSUPPORTED_SIZE;
+    }
+    chain = tmp;
+  }
+  set_factors_from_chain(c, chain, count);
+  cudaStream_t stream = NULL;
+  if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    mofft_core_destroy(c);
+    return MOFFT_INTERNAL_ERROR;
+  }
+  c->stream = stream;
+  mofft_status st = mofft_core_build(c);
+  if (st != MOFFT_SUCCESS) {
+    mofft_core_destroy(c);
+    return st;
+  }
+  *out = c;
+  return MOFFT_SUCCESS;
+}
+
+/* ------------------------------------------------------------------------ */
+/* execute                                                                   */
+/* ------------------------------------------------------------------------ */
+
+static int is_device_pointer(const void *p) {
+  struct cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+/* Enqueue the plan's passes: in -> out on `stream` (device pointers). */
+mofft_status mofft_core_enqueue(const mofft_core *c, const void *in, void *out,
+                                void *stream) {
+  const size_t cb = mofft_complex_bytes(c->precision_bits);
+  const int P = c->sched.pass_count;
+  const int backward = c->direction == MOFFT_BACKWARD;
+  const void *src = in;
+  long long src_dist = (long long)c->distance;
+  for (int p = 0; p < P; ++p) {
+    const mofft_pass *ps = &c->sched.pass[p];
+    void *dst;
+    long long dst_dist;
+    if (p == P - 1) {
+      dst = out;
+      dst_dist = (long long)c->distance;
+    } else if (src != out) {
+      dst = out;
+      dst_dist = (long long)c->distance;
+    } else {
+      if (!c->d_work) return MOFFT_INTERNAL_ERROR;
+      dst = c->d_work;
+      dst_dist = (long long)c->length;
+    }
+    mofft_pass_args a;
+    memset(&a, 0, sizeof(a));
+    a.in = src;
+    a.out = dst;
+    a.tw = (const unsigned char *)c->d_twiddles + ps->tw_offset;
+    a.tw_hi = (const unsigned char *)c->d_twiddles + ps->tw_hi_offset;
+    a.tw_lo = (const unsigned char *)c->d_twiddles + ps->tw_lo_offset;
+    a.batch = (long long)c->batch;
+    a.in_dist = src_dist;
+    a.out_dist = dst_dist;
+    a.total = (long long)c->length;
+    a.ns_outer = ps->ns_outer;
+    a.split_shift = ps->split_shift;
+    a.conj_in = backward && p == 0;
+    a.conj_out = backward && p == P - 1;
+    a.generic_cols = P > 1;
+    a.length = ps->length;
+    a.lines = ps->lines;
+    a.radix_count = ps->radix_count;
+    memcpy(a.radices, ps->radices, sizeof(a.radices));
+    const int err = mofft_cuda_launch_pass(ps->kernel, &a, stream);
+    atomic_fetch_add(&g_launches, 1);
+    if (err != 0) {
+      cudaGetLastError();
+      return MOFFT_INTERNAL_ERROR;
+    }
+    (void)cb;
+    src = dst;
+    src_dist = dst_dist;
+  }
+  return MOFFT_SUCCESS;
+}
+
+static mofft_status ensure_staging(mofft_core *c) {
+  const size_t bytes = c->batch * c->distance * mofft_complex_bytes(c->precision_bits);
+  if (c->stage_bytes >= bytes && c->d_stage[0] && c->d_stage[1])
+    return MOFFT_SUCCESS;
+  if (c->d_stage[0]) cudaFree(c->d_stage[0]);
+  if (c->d_stage[1]) cudaFree(c->d_stage[1]);
+  c->d_stage[0] = c->d_stage[1] = NULL;
+  c->stage_bytes = 0;
+  if (cudaMalloc(&c->d_stage[0], bytes) != cudaSuccess ||
+      cudaMalloc(&c->d_stage[1], bytes) != cudaSuccess) {
+    cudaGetLastError();
+    if (c->d_stage[0]) cudaFree(c->d_stage[0]);
+    c->d_stage[0] = NULL;
+    return MOFFT_ALLOCATION_FAILURE;
+  }
+  c->stage_bytes = bytes;
+  return MOFFT_SUCCESS;
+}
+
+mofft_status mofft_core_execute(const mofft_core *cc, const void *in, void *out) {
+  mofft_core *c = (mofft_core *)cc; /* staging buffers are lazily owned state */
+  if (!c || !in || !out) return MOFFT_INVALID_ARGUMENT;
+  if ((c->placement == MOFFT_IN_PLACE) != (in == out)) return MOFFT_INVALID_ARGUMENT;
+  if (!mofft_hardware_supports(c->precision_bits)) return MOFFT_UNSUPPORTED_HARDWARE;
+  int saved = -1;
+  cudaGetDevice(&saved);
+  if (saved != c->device && cudaSetDevice(c->device) != cudaSuccess) {
+    cudaGetLastError();
+    return MOFFT_INTERNAL_ERROR;
+  }
+  mofft_status st = MOFFT_SUCCESS;
+  const int dev_in = is_device_pointer(in);
+  const int dev_out = in == out ? dev_in : is_device_pointer(out);
+  void *stream = c->user_stream ? c->user_stream : c->stream;
+  if (dev_in && dev_out) {
+    st = mofft_core_enqueue(c, in, out, stream);
+    if (st == MOFFT_SUCCESS && !c->user_stream &&
+        cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) {
+      cudaGetLastError();
+      st = MOFFT_INTERNAL_ERROR;
+    }
+  } else if (dev_in != dev_out) {
+    st = MOFFT_INVALID_ARGUMENT; /* mixed host/device buffers */
+  } else {
+    /* host buffers: stage through plan-owned device memory, blocking */
+    pthread_mutex_lock(&c->lock);
+    st = ensure_staging(c);
+    if (st == MOFFT_SUCCESS) {
+      const size_t cb = mofft_complex_bytes(c->precision_bits);
+      const size_t span = ((c->batch - 1) * c->distance + c->length) * cb;
+      stream = c->stream;
+      if (cudaMemcpyAsync(c->d_stage[0], in, span, cudaMemcpyHostToDevice,
+                          (cudaStream_t)stream) != cudaSuccess)
+        st = MOFFT_INTERNAL_ERROR;
+      if (st == MOFFT_SUCCESS)
+        st = mofft_core_enqueue(c, c->d_stage[0], c->d_stage[1], stream);
+      if (st == MOFFT_SUCCESS &&
+          cudaMemcpyAsync(out, c->d_stage[1], span, cudaMemcpyDeviceToHost,
+                          (cudaStream_t)stream) != cudaSuccess)
+        st = MOFFT_INTERNAL_ERROR;
+      if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess &&
+          st == MOFFT_SUCCESS)
+        st = MOFFT_INTERNAL_ERROR;
+      if (st != MOFFT_SUCCESS) cudaGetLastError();
+    }
+    pthread_mutex_unlock(&c->lock);
+  }
+  if (saved >= 0 && saved != c->device) cudaSetDevice(saved);
+  return st;
+}
+
+uint64_t mofft_launch_count(void) { return (uint64_t)atomic_load(&g_launches); }
+
+/* Schedule the planner would build, without touching a GPU. */
+mofft_status mofft_schedule_preview(int precision_bits, size_t length,
+                                    const int *radices, size_t radix_count,
+                                    unsigned int bank,
+                                    mofft_plan_schedule *out, int *chain_out,
+                                    size_t *chain_count) {
+  if (!out || (precision_bits != 32 && precision_bits != 64) ||
+      bank >= MOFFT_KERNEL_BANK_COUNT)
+    return MOFFT_INVALID_ARGUMENT;
+  if (length < 2 || !mofft_is_smooth13(length)) return MOFFT_UNSUPPORTED_SIZE;
+  int chain[MOFFT_MAX_STAGES];
+  int count;
+  if (radices) {
+    if (radix_count == 0 || radix_count > MOFFT_MAX_STAGES) return MOFFT_INVALID_ARGUMENT;
+    size_t rem = length;
+    for (size_t i = 0; i < radix_count; ++i) {
+      if (!mofft_is_supported_radix(radices[i]) || rem % (size_t)radices[i])
+        return MOFFT_INVALID_ARGUMENT;
+      rem /= (size_t)radices[i];
+    }
+    if (rem != 1) return MOFFT_INVALID_ARGUMENT;
+    count = (int)radix_count;
+    for (int i = 0; i < count; ++i) chain[i] = radices[count - 1 - i];
+  } else {
+    count = mofft_model_chain(precision_bits, bank, length, chain, MOFFT_MAX_STAGES);
+    if (count <= 0) return MOFFT_UNSUPPORTED_SIZE;
+  }
+  mofft_schedule s;
+  if (!mofft_group_chain(precision_bits, bank, chain, count, (long long)length, &s))
+    return MOFFT_UNSUPPORTED_SIZE;
+  memset(out, 0, sizeof(*out));
+  out->pass_count = s.pass_count;
+  for (int p = 0; p < s.pass_count && p < 4; ++p) {
+    out->lengths[p] = s.pass[p].length;
+    out->kernels[p] = s.pass[p].kernel;
+    out->smem_bytes[p] = s.pass[p].smem_bytes;
+  }
+  if (chain_out && chain_count) {
+    /* reference order: outermost radix first */
+    for (int i = 0; i < count; ++i) chain_out[i] = chain[count - 1 - i];
+    *chain_count = (size_t)count;
+  }
+  return MOFFT_SUCCESS;
+}

@@ -1,0 +1,47 @@
+/* Functions shared between the host translation units of libmofft. */
+#ifndef MOFFT_HOST_H
+#define MOFFT_HOST_H
+
+#include "mofft_internal.h"
+
+int mofft_is_supported_radix(int radix);
+int mofft_is_smooth13(size_t n);
+double mofft_monotonic_seconds(void);
+size_t mofft_complex_bytes(int precision_bits);
+int mofft_hardware_supports(int precision_bits);
+int mofft_device_family(uint32_t *family);
+void mofft_cis_turns(uint64_t num, uint64_t den, long double *c,
+                     long double *s);
+
+int mofft_group_chain(int precision_bits, unsigned bank, const int *chain,
+                      int count, long long total, mofft_schedule *best);
+int mofft_auto_radices(long long length, int *out, int capacity);
+int mofft_model_chain(int precision_bits, unsigned bank, size_t length,
+                      int *chain, int capacity);
+
+mofft_status mofft_core_create(mofft_core **out, int precision_bits,
+                               size_t length, size_t batch, size_t distance,
+                               mofft_direction direction,
+                               mofft_placement placement, const int *chain,
+                               int chain_count);
+mofft_status mofft_core_build(mofft_core *c);
+void mofft_core_destroy(mofft_core *c);
+mofft_status mofft_core_enqueue(const mofft_core *c, const void *in, void *out,
+                                void *stream);
+mofft_status mofft_core_execute(const mofft_core *c, const void *in, void *out);
+
+/* MEASURE planner (mofft_measure.c). */
+mofft_status mofft_search_best(mofft_core **out, int precision_bits,
+                               size_t length, size_t batch, size_t distance,
+                               mofft_direction direction,
+                               mofft_placement placement,
+                               const mofft_plan_options *options,
+                               mofft_plan_diagnostics *diagnostics);
+
+/* Compiled wisdom (device plan cache) lookup: returns chain length or 0. */
+int mofft_wisdom_lookup(size_t length, int precision_bits, int *chain,
+                        int capacity);
+
+#define MOFFT_KERNEL_BANK_COUNT 2u
+
+#endif

@@ -1,0 +1,26 @@
+/* Device plan cache: compiled wisdom lookup (the B200 analogue of the
+ * reference's generated mofft_generated_wisdom_lookup,
+ * tools/compile_wisdom.py:98-157).  Entries map (length, precision) to the
+ * tuned Stockham stage chain; the canonical pass grouping turns the chain
+ * into the same device schedule every time. */
+#include <string.h>
+
+#include "generated/wisdom_table.h"
+#include "mofft_host.h"
+
+int mofft_wisdom_lookup(size_t length, int precision_bits, int *chain,
+                        int capacity) {
+  for (int i = 0; i < MOFFT_WISDOM_COUNT; ++i) {
+    const mofft_wisdom_entry *e = &k_mofft_wisdom[i];
+    if (e->length == length && e->precision_bits == precision_bits &&
+        e->count <= capacity) {
+      memcpy(chain, e->chain, (size_t)e->count * sizeof(int));
+      return e->count;
+    }
+  }
+  return 0;
+}
+
+int mofft_wisdom_is_formal(void) { return MOFFT_WISDOM_FORMAL; }
+
+const char *mofft_wisdom_source(void) { return MOFFT_WISDOM_SOURCE; }

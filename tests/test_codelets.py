@@ -1,0 +1,111 @@
+"""Generated CUDA codelets, compiled for the host with g++, against the
+reference's codelet evaluator (golden vectors) -- the role of the reference's
+compiler/mofft_compiler/validate.py candidate harness."""
+from __future__ import annotations
+
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from mofft_b200.codegen import gen_codelets
+from tests.conftest import DBL_EPS, FLT_EPS, ROOT
+
+RADICES = gen_codelets.RADICES
+
+
+HARNESS = r"""
+#define __device__
+#define __forceinline__ inline
+#include <cstdio>
+#include <cstdlib>
+#include "codelets.cuh"
+template <typename T, int R> void run(const double* in, double* out) {
+  T re[R], im[R];
+  for (int i = 0; i < R; ++i) { re[i] = (T)in[2*i]; im[i] = (T)in[2*i+1]; }
+  Dft<R>::fwd(re, im);
+  for (int i = 0; i < R; ++i) { out[2*i] = (double)re[i]; out[2*i+1] = (double)im[i]; }
+}
+template <typename T> void dispatch(int R, const double* in, double* out) {
+  switch (R) {
+#define C(RR) case RR: run<T, RR>(in, out); break;
+    C(2) C(3) C(4) C(5) C(6) C(7) C(8) C(9) C(10) C(11) C(12) C(13) C(14) C(15) C(16) C(32) C(64)
+  }
+}
+int main(int argc, char** argv) {
+  int bits, R;
+  double in[128], out[128];
+  while (scanf("%d %d", &bits, &R) == 2) {
+    for (int i = 0; i < 2 * R; ++i) if (scanf("%lf", &in[i]) != 1) return 1;
+    if (bits == 32) dispatch<float>(R, in, out); else dispatch<double>(R, in, out);
+    for (int i = 0; i < 2 * R; ++i) printf("%.17g ", out[i]);
+    printf("\n");
+  }
+  return 0;
+}
+"""
+
+
+@pytest.fixture(scope="module")
+def harness(tmp_path_factory):
+    d = tmp_path_factory.mktemp("codelets")
+    cuh, _ = gen_codelets.generate()
+    (d / "codelets.cuh").write_text(cuh)
+    (d / "h.cpp").write_text(HARNESS)
+    exe = d / "h"
+    subprocess.run(["g++", "-O1", "-std=c++17", "-ffp-contract=off", "-o", str(exe),
+                    str(d / "h.cpp")], check=True, cwd=d)
+    return exe
+
+
+def run_cases(exe: Path, cases):
+    lines = []
+    for bits, x in cases:
+        vals = " ".join(f"{v:.17g}" for z in x for v in (z.real, z.imag))
+        lines.append(f"{bits} {len(x)} {vals}")
+    out = subprocess.run([str(exe)], input="\n".join(lines) + "\n", capture_output=True,
+                         text=True, check=True).stdout.strip().splitlines()
+    res = []
+    for line in out:
+        v = np.array([float(t) for t in line.split()])
+        res.append(v[0::2] + 1j * v[1::2])
+    return res
+
+
+def test_generated_header_is_current():
+    cuh, costs = gen_codelets.generate()
+    gen = ROOT / "mofft_b200" / "csrc" / "generated"
+    assert (gen / "codelets.cuh").read_text() == cuh
+    assert (gen / "codelet_costs.h").read_text() == costs
+
+
+def test_codelets_match_reference_evaluator(harness, golden_codelets):
+    keys = [k[:-3] for k in golden_codelets.files if k.endswith("_in")]
+    cases, wants, meta = [], [], []
+    for stem in keys:
+        x = golden_codelets[stem + "_in"]
+        want = golden_codelets[stem + "_out"]
+        radix = len(x)
+        backward = "_backward_" in stem
+        for bits in (32, 64):
+            xin = np.conj(x) if backward else x        # bwd(x) = conj(fwd(conj(x)))
+            cases.append((bits, xin))
+            wants.append(want)
+            meta.append((stem, bits, radix, backward))
+    outs = run_cases(harness, cases)
+    assert len(outs) == len(cases)
+    for y, want, (stem, bits, radix, backward) in zip(outs, wants, meta):
+        if backward:
+            y = np.conj(y)
+        tol = 64 * FLT_EPS * radix if bits == 32 else 192 * DBL_EPS * radix
+        assert np.max(np.abs(y - want)) <= tol, (stem, bits)
+
+
+def test_constants_correctly_rounded():
+    c, s = gen_codelets.cis_turns(1, 3)
+    assert c == -0.5 and s == np.sqrt(3) / 2
+    for num, den in [(1, 8), (3, 16), (5, 13), (7, 64)]:
+        c, s = gen_codelets.cis_turns(num, den)
+        assert abs(c - np.cos(2 * np.pi * num / den)) <= 2e-16
+        assert abs(s - np.sin(2 * np.pi * num / den)) <= 2e-16

