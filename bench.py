@@ -63,6 +63,8 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--cpu-seconds", type=float, default=10.0)
+    p.add_argument("--soak", type=float, default=1.0,
+                   help="untimed seconds of the same load before the timed steps")
     return p.parse_args()
 
 
@@ -206,7 +208,7 @@ def cpu_baseline(n: int, bits: int, direction: int, seconds: float) -> dict:
     import oracle
     cores = os.cpu_count() or 1
     dtype = np.complex64 if bits == 32 else np.complex128
-    batch = max(cores, (1 << 21) // n)
+    batch = max(cores, (1 << 22) // n)
     x = oracle.uniform(n * batch, seed=n, dtype=dtype).reshape(batch, n)
     oracle.fft_port(x[:cores], direction, threads=cores)          # warm-up
     samples = []
@@ -215,7 +217,7 @@ def cpu_baseline(n: int, bits: int, direction: int, seconds: float) -> dict:
         t0 = time.perf_counter()
         oracle.fft_port(x, direction, threads=cores)
         samples.append(time.perf_counter() - t0)
-        if len(samples) >= 200:
+        if len(samples) >= 5000:
             break
     med = statistics.median(samples)
     value = flops_per_transform(n) * batch / med / 1e9
@@ -290,23 +292,34 @@ def workload_config(args) -> dict:
 
 # --------------------------------------------------------------- GPU side
 
-def time_device(plan, buf_in, buf_out, steps, warmup, stream, world):
+def time_device(plan, buf_in, buf_out, steps, warmup, stream, world, soak_seconds=0.0):
+    """W untimed warm-up steps, an optional untimed soak (so that the clock
+    samples taken around the timed region see the GPU under this load), then
+    exactly K steps between CUDA events on the plan's stream."""
     import torch
     for _ in range(warmup):
         plan.execute(buf_in, buf_out)
     stream.synchronize()
+    t_end = time.perf_counter() + soak_seconds
+    while time.perf_counter() < t_end:
+        for _ in range(32):
+            plan.execute(buf_in, buf_out)
+        stream.synchronize()
     barrier(world)
     torch.cuda.synchronize()
+    import mofft_b200
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
+    count0 = mofft_b200.launch_count()
     start.record(stream)
     for _ in range(steps):
         plan.execute(buf_in, buf_out)
     end.record(stream)
+    launched = mofft_b200.launch_count() - count0
     end.synchronize()
     torch.cuda.synchronize()
     barrier(world)
-    return start.elapsed_time(end) / steps
+    return start.elapsed_time(end) / steps, launched
 
 
 def run_gpu(args, world, rank, local):
@@ -331,10 +344,9 @@ def run_gpu(args, world, rank, local):
     sched = plan.schedule()
     kernels = {k["index"]: k["name"] for k in m.kernels()}
     # timed region: K steps, device-resident inputs
-    launches0 = m.launch_count()
     with ClockSampler(local) as clocks:
-        ms = time_device(plan, x, y, args.steps, args.warmup, stream, world)
-    launches = m.launch_count() - launches0 - args.warmup * sched["pass_count"]
+        ms, launches = time_device(plan, x, y, args.steps, args.warmup, stream, world,
+                                   soak_seconds=args.soak)
     ms_max = max_over_ranks(ms, world)
     flops = flops_per_transform(n) * batch
     value = flops * world / (ms_max / 1e3) / 1e9
@@ -427,7 +439,7 @@ def run_sweep(args, world, rank, local):
             plan = m.Plan.create(n, args.direction, m.IN_PLACE, bits=bits, batch=batch)
             stream = torch.cuda.Stream()
             plan.set_stream(stream.cuda_stream)
-            ms = time_device(plan, x, x, 10, 3, stream, world)
+            ms, _ = time_device(plan, x, x, 10, 3, stream, world)
             sched = plan.schedule()
             plan.destroy()
             cb = 8 if bits == 32 else 16
