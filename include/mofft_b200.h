@@ -71,6 +71,36 @@ mofft_status mofft_schedule_preview(int precision_bits, size_t length,
                                     mofft_plan_schedule *schedule,
                                     int *chain_out, size_t *chain_count);
 
+/* Allocation-free execution (no counterpart in the reference).
+ *
+ * For callers that cannot allocate device memory: code embedded in a host
+ * framework that reserves the whole GPU memory budget up front and forbids
+ * further cudaMalloc calls, and latency-critical loops where a cudaMalloc /
+ * cudaFree (which may synchronize the device) is not acceptable.  Plans
+ * allocate at creation; this call allocates nothing.  It runs a batched FP32
+ * transform whose schedule has two passes (four-step: lengths beyond one
+ * CTA's shared memory, e.g. 2^15..2^22) from the device buffer `input` to
+ * the device buffer `output` (they may be equal), enqueued on `stream` (a
+ * cudaStream_t, NULL for the default stream); the call returns without
+ * waiting.  The intermediate array and its twiddle tables live in a static
+ * device array of MOFFT_FIXED_SCRATCH_POINTS complex values (32 MiB plus 512
+ * KiB of twiddles) that every GPU loading the library holds until exit.
+ *
+ * Limits: batch * length <= MOFFT_FIXED_SCRATCH_POINTS, else
+ * MOFFT_UNSUPPORTED_SIZE; lengths that run in one pass (they need no scratch)
+ * or in three, also MOFFT_UNSUPPORTED_SIZE; host buffers give
+ * MOFFT_INVALID_ARGUMENT.  The first call on each device sets up the array's
+ * device address (with that device current), so make that first call before
+ * any stream capture on that device.  All calls share the array and it keeps
+ * the last call's contents; calls whose executions overlap on the GPU race on
+ * it, so order them (for example on one stream). */
+#define MOFFT_FIXED_SCRATCH_POINTS (1u << 22)
+mofft_status mofft_execute_fixed_scratch_f32(const mofft_complex_f32 *input,
+                                             mofft_complex_f32 *output,
+                                             size_t length, size_t batch,
+                                             mofft_direction direction,
+                                             void *stream);
+
 /* Kernel registry introspection. */
 int mofft_kernel_count(void);
 /* Fills name (NUL-terminated, truncated to capacity) and shape of entry i;

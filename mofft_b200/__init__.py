@@ -153,6 +153,7 @@ _PLAIN = [
                                ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I),
                                ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     ("mofft_launch_count", _U64, []),
+    ("mofft_execute_fixed_scratch_f32", _I, [_P, _P, _SZ, _SZ, _I, _P]),
     ("mofft_schedule_preview", _I, [_I, _SZ, ctypes.POINTER(_I), _SZ, ctypes.c_uint,
                                     ctypes.POINTER(Schedule), ctypes.POINTER(_I),
                                     ctypes.POINTER(_SZ)]),

@@ -4,6 +4,10 @@
 
 #include "mofft_internal.h"
 
+#ifdef __cplusplus
+extern "C" {
+#endif
+
 int mofft_is_supported_radix(int radix);
 int mofft_is_smooth13(size_t n);
 double mofft_monotonic_seconds(void);
@@ -44,4 +48,7 @@ int mofft_wisdom_lookup(size_t length, int precision_bits, int *chain,
 
 #define MOFFT_KERNEL_BANK_COUNT 2u
 
+#ifdef __cplusplus
+}
+#endif
 #endif
