@@ -182,13 +182,22 @@ def barrier(world):
 
 
 def max_over_ranks(value: float, world: int) -> float:
+    """Max of a per-rank timing over all ranks (NCCL on GPUs, gloo on CPU)."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(flops_per_rank: float, ms_per_rank: float, world: int) -> tuple[float, float]:
+    """Whole-job GFLOP/s of `world` replicas: all ranks' work over the slowest
+    rank's time.  Returns (GFLOP/s, max ms)."""
+    ms_max = max_over_ranks(ms_per_rank, world)
+    return flops_per_rank * world / (ms_max / 1e3) / 1e9, ms_max
 
 
 def dist_teardown(world):
@@ -347,9 +356,8 @@ def run_gpu(args, world, rank, local):
     with ClockSampler(local) as clocks:
         ms, launches = time_device(plan, x, y, args.steps, args.warmup, stream, world,
                                    soak_seconds=args.soak)
-    ms_max = max_over_ranks(ms, world)
     flops = flops_per_transform(n) * batch
-    value = flops * world / (ms_max / 1e3) / 1e9
+    value, ms_max = replica_value(flops, ms, world)
     # roofline of the dominant kernel (per-pass timing when the plan has several)
     peak, peak_kind = measured_peaks()
     p_alg = passes_for(n, bits)

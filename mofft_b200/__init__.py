@@ -221,7 +221,9 @@ def kernels() -> list[dict]:
         bits, kind, length, lines, threads, count = (v.value for v in vals)
         out.append({"index": i, "name": name.value.decode(), "precision_bits": bits,
                     "kind": kind, "length": length, "lines": lines, "threads": threads,
-                    "radices": list(rad[:count])})
+                    "radices": list(rad[:count]),
+                    # generic kernels record the largest radix they run
+                    "max_radix": rad[0] if kind == KERNEL_GENERIC else max(rad[:count])})
     return out
 
 

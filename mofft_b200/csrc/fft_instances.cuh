@@ -126,10 +126,10 @@ size_t generic_smem(int L, int lines, int cols) {
   return 4 * words * sizeof(T);
 }
 
-template <typename T>
+template <typename T, bool WIDE>
 struct GenericInst {
   static const void *func() {
-    return reinterpret_cast<const void *>(&generic_kernel<T>);
+    return reinterpret_cast<const void *>(&generic_kernel<T, WIDE>);
   }
   static cudaError_t launch(const mofft_pass_args *p, cudaStream_t s) {
     GenericArgs<T> a;
@@ -156,6 +156,8 @@ struct GenericInst {
       if (i < p->radix_count) prod *= p->radices[i];
     }
     if (prod != p->length) return cudaErrorInvalidValue;
+    for (int i = 0; i < p->radix_count; ++i)
+      if (!WIDE && p->radices[i] > 16) return cudaErrorInvalidValue;
     a.sign_in = p->conj_in ? T(-1) : T(1);
     a.sign_out = p->conj_out ? T(-1) : T(1);
     long long grid;
@@ -170,7 +172,7 @@ struct GenericInst {
     if (grid <= 0) return cudaSuccess;
     if (grid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     const size_t smem = generic_smem<T>(p->length, p->lines, p->generic_cols);
-    generic_kernel<T><<<(unsigned)grid, 256, smem, s>>>(a);
+    generic_kernel<T, WIDE><<<(unsigned)grid, 256, smem, s>>>(a);
     return cudaGetLastError();
   }
   static Entry entry(const char *name) {
@@ -182,8 +184,10 @@ struct GenericInst {
     e.desc.lines = 0;
     e.desc.threads = 256;
     e.desc.staged = 0;
+    // radices[0] records the largest radix this variant runs
     e.desc.radix_count = 0;
     for (int i = 0; i < 8; ++i) e.desc.radices[i] = 0;
+    e.desc.radices[0] = WIDE ? 64 : 16;
     e.desc.smem_bytes = 227 * 1024;
     e.launch = &launch;
     e.func = &func;
@@ -203,5 +207,7 @@ const Entry *entries_rows_f32(int *count);
 const Entry *entries_rows_f64(int *count);
 const Entry *entries_cols_f32(int *count);
 const Entry *entries_cols_f64(int *count);
+const Entry *entries_rows_mixed(int *count);
+const Entry *entries_cols_mixed(int *count);
 
 }  // namespace mofft

@@ -4,8 +4,10 @@
 namespace mofft {
 const Entry *entries_generic(int *count) {
   static const Entry e[] = {
-      GenericInst<float>::entry("generic_float"),
-      GenericInst<double>::entry("generic_double"),
+      GenericInst<float, false>::entry("generic_float"),
+      GenericInst<double, false>::entry("generic_double"),
+      GenericInst<float, true>::entry("generic_float_wide"),
+      GenericInst<double, true>::entry("generic_double_wide"),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;

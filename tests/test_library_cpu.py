@@ -171,7 +171,9 @@ def test_cost_model_reference_accounting():
 
 def test_kernel_registry_is_consistent():
     ks = m.kernels()
-    assert sum(k["kind"] == m.KERNEL_GENERIC for k in ks) == 2
+    generic = [k for k in ks if k["kind"] == m.KERNEL_GENERIC]
+    assert sorted((k["precision_bits"], k["max_radix"]) for k in generic) == \
+        [(32, 16), (32, 64), (64, 16), (64, 64)]
     for k in ks:
         if k["kind"] == m.KERNEL_GENERIC:
             continue
@@ -179,9 +181,24 @@ def test_kernel_registry_is_consistent():
         assert k["threads"] <= 1024 and k["threads"] % 32 == 0 or k["threads"] < 32 or \
             k["threads"] % 8 == 0
     for bits in (32, 64):
-        for e in range(1, 14 if bits == 32 else 13):
-            assert any(k["kind"] == m.KERNEL_ROWS and k["length"] == 2 ** e and
-                       k["precision_bits"] == bits for k in ks), (bits, e)
+        lengths = [2 ** e for e in range(1, 14 if bits == 32 else 13)] + \
+            [3 * 2 ** e for e in range(4, 13)] + [5 * 2 ** e for e in range(4, 12)]
+        for n in lengths:
+            assert any(k["kind"] == m.KERNEL_ROWS and k["length"] == n and
+                       k["precision_bits"] == bits for k in ks), (bits, n)
+
+
+def test_mixed_lengths_use_specialised_kernels():
+    """3*2^k and 5*2^k lengths of the plain-method sweep run on specialised
+    kernels (no runtime-stage kernel), single pass up to 12288 / 10240."""
+    ks = {k["index"]: k for k in m.kernels()}
+    for bits in (32, 64):
+        for n in [3 * 2 ** e for e in range(4, 19)] + [5 * 2 ** e for e in range(4, 18)]:
+            s = m.schedule_preview(n, bits)
+            kinds = [ks[k]["kind"] for k in s["kernels"]]
+            assert m.KERNEL_GENERIC not in kinds, (bits, n, s)
+            if n <= 12288:
+                assert s["pass_count"] == 1, (bits, n, s)
 
 
 SWEEP = [2 ** e for e in range(1, 25)] + [3 * 2 ** e for e in range(4, 19)] + \
