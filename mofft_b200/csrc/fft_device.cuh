@@ -58,8 +58,11 @@ __device__ __forceinline__ void cmul(T& xr, T& xi, T wr, T wi) {
   xi = i;
 }
 
+// Data is read once: load through L2 only (ld.global.cg), which also keeps
+// reads coherent with writes of other CTAs of the same launch (the ragged
+// persistent kernel reads its second pass after a device-scope fence).
 template <typename T>
-__device__ __forceinline__ cplx_t<T> ld_global(const cplx_t<T>* p) { return *p; }
+__device__ __forceinline__ cplx_t<T> ld_global(const cplx_t<T>* p) { return __ldcg(p); }
 template <typename T>
 __device__ __forceinline__ void st_global(cplx_t<T>* p, T re, T im) {
   cplx_t<T> v;
@@ -263,17 +266,17 @@ struct RowsArgs {
   T sign;
 };
 
+// Body of one ROWS tile: transforms b0 .. b0+TB-1, run by threads
+// 0 .. TPL*TB-1 of the CTA (every thread of the CTA must call it).
 template <typename T, int L, int TPL, int TB, bool STAGED, int... Rs>
-__global__ void __launch_bounds__(TPL * TB)
-rows_kernel(const RowsArgs<T> a) {
+__device__ __forceinline__ void rows_body(const RowsArgs<T>& a, long long b0,
+                                          unsigned char* smem_raw) {
   static_assert(StageProduct<L, Rs...>::value == L, "radices must multiply to L");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int LINE = spad_len<T>(L);
   T* sre = reinterpret_cast<T*>(smem_raw);
   T* sim = sre + TB * LINE;
   const int line = threadIdx.x / TPL;
   const int t = threadIdx.x % TPL;
-  const long long b0 = (long long)blockIdx.x * TB;
   const long long b = b0 + line;
   RowsLayout<T> lay;
   lay.sre = sre + line * LINE;
@@ -310,6 +313,13 @@ rows_kernel(const RowsArgs<T> a) {
   }
 }
 
+template <typename T, int L, int TPL, int TB, bool STAGED, int... Rs>
+__global__ void __launch_bounds__(TPL * TB)
+rows_kernel(const RowsArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  rows_body<T, L, TPL, TB, STAGED, Rs...>(a, (long long)blockIdx.x * TB, smem_raw);
+}
+
 // ---------------------------------------------------------------------------
 // COLS kernel: one pass of a multi-pass transform of total length M.
 // Lines are the super-butterflies j in [0, M/L); a CTA owns C consecutive
@@ -343,18 +353,16 @@ struct ColsGeom {
   static constexpr int THREADS = TPL * C;
 };
 
+// Body of one COLS tile: lines j0 .. j0+C-1 of batch entry b, run by threads
+// 0 .. TPL*C-1 of the CTA (every thread of the CTA must call it).
 template <typename T, int L, int TPL, int C, int... Rs>
-__global__ void __launch_bounds__(TPL * C)
-cols_kernel(const ColsArgs<T> a) {
+__device__ __forceinline__ void cols_body(const ColsArgs<T>& a, long long b,
+                                          long long j0, unsigned char* smem_raw) {
   static_assert(StageProduct<L, Rs...>::value == L, "radices must multiply to L");
   using G = ColsGeom<T, L, TPL, C>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sre = reinterpret_cast<T*>(smem_raw);
   T* sim = sre + G::WORDS;
   const long long lines_total = a.total / L;            // M / L
-  const long long groups = lines_total / C;             // C divides M/L
-  const long long b = blockIdx.x / groups;
-  const long long j0 = (blockIdx.x - b * groups) * C;
   const int c = threadIdx.x % C;
   const int t = threadIdx.x / C;
   const long long j = j0 + c;
@@ -391,6 +399,16 @@ cols_kernel(const ColsArgs<T> a) {
   } else {
     StageRunner<T, L, TPL, 1, 0, false, false, true, Rs...>::run(lay, t, a.tw);
   }
+}
+
+template <typename T, int L, int TPL, int C, int... Rs>
+__global__ void __launch_bounds__(TPL * C)
+cols_kernel(const ColsArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const long long groups = (a.total / L) / C;           // C divides M/L
+  const long long b = blockIdx.x / groups;
+  const long long j0 = (blockIdx.x - b * groups) * C;
+  cols_body<T, L, TPL, C, Rs...>(a, b, j0, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -495,7 +513,10 @@ __device__ __forceinline__ void generic_butterfly(
   }
 }
 
-template <typename T>
+// WIDE selects the variant that also handles radix 32 and 64; chains without
+// them use the narrow variant, whose register footprint allows several CTAs
+// per SM.
+template <typename T, bool WIDE>
 __device__ __forceinline__ void generic_dispatch(
     int R, const GenericArgs<T>& a, const T* sre_src, const T* sim_src,
     T* sre_dst, T* sim_dst, int line, int j, int L, int NS, int twoff,
@@ -511,14 +532,22 @@ __device__ __forceinline__ void generic_dispatch(
     MOFFT_GENERIC_CASE(8) MOFFT_GENERIC_CASE(9) MOFFT_GENERIC_CASE(10)
     MOFFT_GENERIC_CASE(11) MOFFT_GENERIC_CASE(12) MOFFT_GENERIC_CASE(13)
     MOFFT_GENERIC_CASE(14) MOFFT_GENERIC_CASE(15) MOFFT_GENERIC_CASE(16)
-    MOFFT_GENERIC_CASE(32) MOFFT_GENERIC_CASE(64)
-    default: break;
+    default:
+      if (WIDE) {
+        if (R == 32)
+          generic_butterfly<T, 32>(a, sre_src, sim_src, sre_dst, sim_dst, line, j, L,
+                                   NS, twoff, first, last, line_words, b, jline);
+        else if (R == 64)
+          generic_butterfly<T, 64>(a, sre_src, sim_src, sre_dst, sim_dst, line, j, L,
+                                   NS, twoff, first, last, line_words, b, jline);
+      }
+      break;
   }
 #undef MOFFT_GENERIC_CASE
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) generic_kernel(const GenericArgs<T> a) {
+template <typename T, bool WIDE>
+__global__ void __launch_bounds__(256, WIDE ? 1 : 2) generic_kernel(const GenericArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int L = a.length;
   const bool cols = a.cols != 0;
@@ -560,7 +589,7 @@ __global__ void __launch_bounds__(256) generic_kernel(const GenericArgs<T> a) {
       const long long bb = cols ? b : b + line;
       if (bb >= a.batch) continue;
       const long long jline = cols ? jfirst + line : 0;
-      generic_dispatch<T>(R, a, bufs[cur][0], bufs[cur][1], bufs[cur ^ 1][0],
+      generic_dispatch<T, WIDE>(R, a, bufs[cur][0], bufs[cur][1], bufs[cur ^ 1][0],
                           bufs[cur ^ 1][1], line, j, L, NS, twoff, first, last,
                           line_words, cols ? b : bb, jline);
     }

@@ -151,8 +151,8 @@ void mofft_cis_turns(uint64_t num, uint64_t den, long double *c,
 
 /* Writes count forward twiddles W_den^(e) = exp(-2 pi i e/den) for
  * e = first + k*step into dst (precision_bits wide complex). */
-static void write_twiddles(void *dst, int precision_bits, uint64_t den,
-                           uint64_t first, uint64_t step, size_t count) {
+void mofft_write_twiddles(void *dst, int precision_bits, uint64_t den,
+                          uint64_t first, uint64_t step, size_t count) {
   for (size_t k = 0; k < count; ++k) {
     long double c, s;
     mofft_cis_turns((first + (uint64_t)k * step) % den, den, &c, &s);
@@ -168,7 +168,7 @@ static void write_twiddles(void *dst, int precision_bits, uint64_t den,
 
 /* Internal stage table of an in-CTA chain: stage (R, Ns>1) stores
  * W_{Ns*R}^{jm*r} at (r-1)*Ns + jm. */
-static size_t stage_table_entries(const int *radices, int count) {
+size_t mofft_stage_table_entries(const int *radices, int count) {
   size_t total = 0, ns = 1;
   for (int i = 0; i < count; ++i) {
     if (ns > 1) total += (size_t)(radices[i] - 1) * ns;
@@ -177,8 +177,8 @@ static size_t stage_table_entries(const int *radices, int count) {
   return total;
 }
 
-static void fill_stage_table(void *dst, int precision_bits, const int *radices,
-                             int count) {
+void mofft_fill_stage_table(void *dst, int precision_bits, const int *radices,
+                            int count) {
   const size_t cb = mofft_complex_bytes(precision_bits);
   unsigned char *p = (unsigned char *)dst;
   size_t ns = 1;
@@ -186,7 +186,7 @@ static void fill_stage_table(void *dst, int precision_bits, const int *radices,
     const size_t R = (size_t)radices[i];
     if (ns > 1) {
       for (size_t r = 1; r < R; ++r) {
-        write_twiddles(p, precision_bits, ns * R, 0, r, ns);
+        mofft_write_twiddles(p, precision_bits, ns * R, 0, r, ns);
         p += ns * cb;
       }
     }
@@ -194,7 +194,7 @@ static void fill_stage_table(void *dst, int precision_bits, const int *radices,
   }
 }
 
-static int ceil_log2_u64(uint64_t x) {
+int mofft_ceil_log2_u64(uint64_t x) {
   int s = 0;
   while (((uint64_t)1 << s) < x) ++s;
   return s;
@@ -206,14 +206,24 @@ static int ceil_log2_u64(uint64_t x) {
 
 #define SMEM_LIMIT (227u * 1024u)
 
-static int generic_kernel_index(int precision_bits) {
+/* Generic (runtime stage list) kernel that can run every radix of `chain`:
+ * the narrow variant (radix <= 16) when possible, else the wide one. */
+static int generic_kernel_index(int precision_bits, const int *chain, int count) {
+  int max_radix = 0;
+  for (int i = 0; i < count; ++i)
+    if (chain[i] > max_radix) max_radix = chain[i];
+  int best = -1, best_cap = 1 << 30;
   const int n = mofft_cuda_kernel_count();
   for (int i = 0; i < n; ++i) {
     const mofft_kernel_desc *d = mofft_cuda_kernel_get(i);
-    if (d->kind == MOFFT_KERNEL_GENERIC && d->precision_bits == precision_bits)
-      return i;
+    if (d->kind != MOFFT_KERNEL_GENERIC || d->precision_bits != precision_bits) continue;
+    const int cap = d->radices[0];
+    if (cap >= max_radix && cap < best_cap) {
+      best = i;
+      best_cap = cap;
+    }
   }
-  return -1;
+  return best;
 }
 
 static int chain_equal(const int *a, int na, const int *b, int nb) {
@@ -315,7 +325,7 @@ static int make_pass(int precision_bits, unsigned bank, const int *chain,
       return 1;
     }
   }
-  const int g = generic_kernel_index(precision_bits);
+  const int g = generic_kernel_index(precision_bits, chain + begin, count);
   if (g < 0) return 0;
   int lines = single ? generic_rows_lines(precision_bits, (int)length)
                      : generic_cols_lines(precision_bits, (int)length, total,
@@ -539,12 +549,12 @@ static mofft_status materialise_schedule(mofft_core *c) {
   for (int p = 0; p < c->sched.pass_count; ++p) {
     mofft_pass *ps = &c->sched.pass[p];
     ps->tw_offset = bytes;
-    bytes = align256(bytes + stage_table_entries(ps->radices, ps->radix_count) * cb + cb);
+    bytes = align256(bytes + mofft_stage_table_entries(ps->radices, ps->radix_count) * cb + cb);
     ps->split_shift = 0;
     ps->tw_hi_offset = ps->tw_lo_offset = bytes;
     if (ps->ns_outer > 1) {
       const uint64_t m = (uint64_t)ps->ns_outer * (uint64_t)ps->length;
-      const int shift = (ceil_log2_u64(m) + 1) / 2;
+      const int shift = (mofft_ceil_log2_u64(m) + 1) / 2;
       ps->split_shift = shift;
       const size_t lo_n = (size_t)1 << shift;
       const size_t hi_n = (size_t)((m + lo_n - 1) >> shift);
@@ -559,14 +569,14 @@ static mofft_status materialise_schedule(mofft_core *c) {
   if (!host) return MOFFT_ALLOCATION_FAILURE;
   for (int p = 0; p < c->sched.pass_count; ++p) {
     const mofft_pass *ps = &c->sched.pass[p];
-    fill_stage_table(host + ps->tw_offset, c->precision_bits, ps->radices,
+    mofft_fill_stage_table(host + ps->tw_offset, c->precision_bits, ps->radices,
                      ps->radix_count);
     if (ps->ns_outer > 1) {
       const uint64_t m = (uint64_t)ps->ns_outer * (uint64_t)ps->length;
       const size_t lo_n = (size_t)1 << ps->split_shift;
       const size_t hi_n = (size_t)((m + lo_n - 1) >> ps->split_shift);
-      write_twiddles(host + ps->tw_hi_offset, c->precision_bits, m, 0, lo_n, hi_n);
-      write_twiddles(host + ps->tw_lo_offset, c->precision_bits, m, 0, 1, lo_n);
+      mofft_write_twiddles(host + ps->tw_hi_offset, c->precision_bits, m, 0, lo_n, hi_n);
+      mofft_write_twiddles(host + ps->tw_lo_offset, c->precision_bits, m, 0, 1, lo_n);
     }
   }
   release_device(c);
@@ -814,6 +824,8 @@ mofft_status mofft_core_execute(const mofft_core *cc, const void *in, void *out)
 }
 
 uint64_t mofft_launch_count(void) { return (uint64_t)atomic_load(&g_launches); }
+
+void mofft_count_launches(uint64_t n) { atomic_fetch_add(&g_launches, n); }
 
 /* Schedule the planner would build, without touching a GPU. */
 mofft_status mofft_schedule_preview(int precision_bits, size_t length,

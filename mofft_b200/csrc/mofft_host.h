@@ -34,6 +34,17 @@ mofft_status mofft_core_enqueue(const mofft_core *c, const void *in, void *out,
                                 void *stream);
 mofft_status mofft_core_execute(const mofft_core *c, const void *in, void *out);
 
+/* Twiddle tables (mofft_api.c): W_den^(first + k*step), k < count; the
+ * internal stage table of an in-CTA chain; ceil(log2 x). */
+void mofft_write_twiddles(void *dst, int precision_bits, uint64_t den,
+                          uint64_t first, uint64_t step, size_t count);
+size_t mofft_stage_table_entries(const int *radices, int count);
+void mofft_fill_stage_table(void *dst, int precision_bits, const int *radices,
+                            int count);
+int mofft_ceil_log2_u64(uint64_t x);
+/* Adds n to the process-wide libmofft launch counter. */
+void mofft_count_launches(uint64_t n);
+
 /* MEASURE planner (mofft_measure.c). */
 mofft_status mofft_search_best(mofft_core **out, int precision_bits,
                                size_t length, size_t batch, size_t distance,
