@@ -48,6 +48,8 @@ if str(ROOT) not in sys.path:
 FALLBACK_HBM_GBS = 6650.0
 
 
+FORMS = {"fp32": 0, "tf32x3": 1, "bf16x3": 2}   # mofft_precision_form
+
 def parse_args():
     p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     p.add_argument("--gpus", type=int, default=1)
@@ -59,7 +61,15 @@ def parse_args():
     p.add_argument("--points", type=int, default=1 << 26, help="points per call per GPU")
     p.add_argument("--direction", type=int, choices=[-1, 1], default=-1)
     p.add_argument("--out-of-place", action="store_true")
+    p.add_argument("--form", choices=list(FORMS), default="fp32",
+                   help="precision form of the FP32 plan (tensor-core forms: n=4096)")
     p.add_argument("--sweep", action="store_true")
+    p.add_argument("--serve", action="store_true",
+                   help="serving stream: continuous batching vs serial per-request execution")
+    p.add_argument("--requests", type=int, default=600,
+                   help="requests of the seeded serving stream (bounded sample)")
+    p.add_argument("--ragged", action="store_true",
+                   help="ragged batch: 512 mixed FP32 transforms, persistent launch vs per item")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -296,7 +306,7 @@ def workload_config(args) -> dict:
             "n": n, "batch": batch, "precision_bits": args.bits,
             "placement": "out-of-place" if args.out_of_place else "in-place",
             "inputs": "uniform[-1,1) seeded; 2^26-point working set > L2 (no flush)",
-            "parallelism": f"replicas x{args.gpus}"}
+            "parallelism": f"replicas x{args.gpus}", "form": args.form}
 
 
 # --------------------------------------------------------------- GPU side
@@ -348,6 +358,7 @@ def run_gpu(args, world, rank, local):
     y = x if inplace else torch.empty_like(x)
     plan = m.Plan.create(n, args.direction, m.IN_PLACE if inplace else m.OUT_OF_PLACE,
                          bits=bits, batch=batch)
+    apply_form(plan, args)
     stream = torch.cuda.Stream()
     plan.set_stream(stream.cuda_stream)
     sched = plan.schedule()
@@ -370,7 +381,8 @@ def run_gpu(args, world, rank, local):
     dom_bytes = 2 * cb * n * batch  # each pass reads and writes every point once
     achieved = dom_bytes / (pass_ms[dom] / 1e3) / 1e9
     workload = f"n={n} batch={batch} fp{bits}"
-    traffic = committed_traffic(kernels[sched["kernels"][dom]], workload)
+    entry = committed_traffic(kernels[sched["kernels"][dom]], workload)
+    traffic = entry["bytes"] if entry else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": traffic, "peak_source": f"of {peak_kind}",
@@ -395,6 +407,11 @@ def run_gpu(args, world, rank, local):
     return line
 
 
+def apply_form(plan, args):
+    if args.form != "fp32":
+        plan.set_precision_form(FORMS[args.form])
+
+
 def per_pass_times(plan, x, y, stream, sched):
     """Kernel time of each pass, measured with events on the plan's stream by
     running one-pass plans of the same decomposition is not possible from the
@@ -416,6 +433,7 @@ def run_e2e(args, m, n, bits, batch, x_dev):
     h_out = torch.empty_like(h_in, pin_memory=True)
     h_in.copy_(x_dev)
     plan = m.Plan.create(n, args.direction, m.OUT_OF_PLACE, bits=bits, batch=batch)
+    apply_form(plan, args)
     plan.execute(h_in, h_out)  # warm-up (allocates the staging buffers)
     times = []
     for _ in range(max(1, args.e2e_steps)):
@@ -445,6 +463,7 @@ def run_sweep(args, world, rank, local):
             real_t = torch.float32 if bits == 32 else torch.float64
             x = torch.view_as_complex(torch.rand((batch, n, 2), device="cuda", dtype=real_t))
             plan = m.Plan.create(n, args.direction, m.IN_PLACE, bits=bits, batch=batch)
+            apply_form(plan, args)
             stream = torch.cuda.Stream()
             plan.set_stream(stream.cuda_stream)
             ms, _ = time_device(plan, x, x, 10, 3, stream, world)
@@ -463,6 +482,206 @@ def run_sweep(args, world, rank, local):
             torch.cuda.empty_cache()
 
 
+def run_ragged(args, world, rank, local):
+    """512 FP32 transforms of mixed length / batch / direction (seed 7): one
+    persistent launch from a CUDA graph vs one plain launch per transform
+    (eager, and captured in a CUDA graph)."""
+    import torch
+
+    import mofft_b200 as m
+    from mofft_b200 import workloads
+    torch.cuda.set_device(local)
+    spec = workloads.ragged_spec(count=512, seed=7)
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    items, flops, points = [], 0.0, 0
+    for n, batch, direction in spec:
+        x = torch.view_as_complex(torch.rand((batch, n, 2), generator=gen, device="cuda") * 2 - 1)
+        items.append((x, torch.empty_like(x), direction))
+        flops += flops_per_transform(n) * batch
+        points += n * batch
+    plan = m.RaggedPlan(items)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+
+    def timed(fn, reps):
+        for _ in range(3):
+            fn()
+        stream.synchronize()
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(reps):
+            fn()
+        e.record(stream)
+        e.synchronize()
+        return s.elapsed_time(e) / reps
+
+    ragged_ms = timed(lambda: plan.execute(sh), args.steps)
+    assert plan.status() == 0, "ragged kernel reported a timed-out dependency wait"
+    per_item_ms = timed(lambda: plan.execute_per_item(sh), max(3, args.steps // 4))
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(stream):
+        plan.execute_per_item(sh)
+        stream.synchronize()
+        with torch.cuda.graph(graph, stream=stream):
+            plan.execute_per_item(torch.cuda.current_stream().cuda_stream)
+    def replay():
+        with torch.cuda.stream(stream):
+            graph.replay()
+
+    graph_ms = timed(replay, max(3, args.steps // 4))
+    tiles, grid = plan.info()
+    peak, kind = measured_peaks()
+    line = {
+        "metric": "ragged C2C GFLOP/s (5n log2 n)", "value": round(flops / ragged_ms / 1e6, 1),
+        "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": 3,
+        "ms_per_step": round(ragged_ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "ragged: 512 transforms, n in {2^6..2^16} U {3*2^5..3*2^13}, "
+                               "batch 1..64, mixed directions, seed 7",
+                   "points": points, "tiles": tiles, "persistent_ctas": grid},
+        "per_item_eager": {"ms": round(per_item_ms, 4),
+                           "gflops": round(flops / per_item_ms / 1e6, 1)},
+        "per_item_graph": {"ms": round(graph_ms, 4), "gflops": round(flops / graph_ms / 1e6, 1)},
+        "speedup_vs_per_item_graph": round(graph_ms / ragged_ms, 2),
+        "hbm_frac_one_pass_bytes": round(points * 16 / (ragged_ms / 1e3) / 1e9 / peak, 3),
+    }
+    del graph
+    plan.destroy()
+    return line
+
+
+def run_serve(args, world, rank, local):
+    """Serving stream (seeded): n Zipf(1.1) over 2^8..2^20, batch 1..256,
+    80 % FP32 / 20 % FP64, device-resident payloads.  The server (continuous
+    batching, 4 streams, 40 GiB admission) and serial plain execution (one
+    blocking plan execute per request, plans created beforehand) process the
+    same requests: all at t=0 (saturation) and at Poisson rates of 50 % and
+    90 % of the serial capacity."""
+    import threading
+
+    import numpy as np
+    import torch
+
+    import mofft_b200 as m
+    from mofft_b200 import workloads
+    torch.cuda.set_device(local)
+    reqs = workloads.serving_stream(args.requests, rate_per_s=1.0, seed=11)
+    maxpts = max(r["n"] * r["batch"] for r in reqs)
+    arena_in = {32: torch.view_as_complex(torch.rand((maxpts, 2), device="cuda") * 2 - 1),
+                64: torch.view_as_complex(torch.rand((maxpts, 2), device="cuda",
+                                                     dtype=torch.float64) * 2 - 1)}
+    ring_bytes = 24 << 30
+    ring = torch.empty(ring_bytes // 16, dtype=torch.complex128, device="cuda")
+    flops = [flops_per_transform(r["n"]) * r["batch"] for r in reqs]
+    total_flops = sum(flops)
+
+    def out_ptr(offset):
+        return ring.data_ptr() + offset
+
+    # serial plain per-request execution: one cached batched plan per shape
+    plans = {}
+    for r in reqs:
+        key = (r["n"], r["batch"], r["direction"], r["bits"])
+        if key not in plans:
+            plans[key] = m.Plan.create(r["n"], r["direction"], m.OUT_OF_PLACE, bits=r["bits"],
+                                       batch=r["batch"])
+
+    def run_serial(arrivals):
+        lat = []
+        t0 = time.perf_counter()
+        offset = 0
+        for r, a in zip(reqs, arrivals):
+            now = time.perf_counter() - t0
+            if a > now:
+                time.sleep(a - now)
+            nbytes = r["n"] * r["batch"] * (8 if r["bits"] == 32 else 16)
+            if offset + nbytes > ring_bytes:
+                offset = 0
+            st = plans[(r["n"], r["batch"], r["direction"], r["bits"])].execute_ptr(
+                arena_in[r["bits"]].data_ptr(), out_ptr(offset))
+            assert st == 0
+            offset += nbytes
+            lat.append(time.perf_counter() - t0 - a)
+        return time.perf_counter() - t0, lat
+
+    def run_server(arrivals):
+        srv = m.Server(hbm_budget_bytes=40 << 30, streams=4)
+        # warm the server's plan cache outside the timed run
+        for key in {(r["n"], r["direction"], r["bits"]) for r in reqs}:
+            srv.wait(srv.submit(key[0], 1, key[1], key[2], arena_in[key[2]].data_ptr(),
+                                out_ptr(0)))
+        tickets = []
+        lat_of = {}
+        inflight = []          # (ticket, bytes) in ring order: client flow control
+        used = 0
+        t0 = time.perf_counter()
+        offset = 0
+        for r, a in zip(reqs, arrivals):
+            now = time.perf_counter() - t0
+            if a > now:
+                time.sleep(a - now)
+            nbytes = r["n"] * r["batch"] * (8 if r["bits"] == 32 else 16)
+            while inflight and used + nbytes > ring_bytes // 2:
+                t, b = inflight.pop(0)
+                lat_of[t] = srv.wait(t)[1]
+                used -= b
+            if offset + nbytes > ring_bytes:
+                offset = 0
+            t = srv.submit(r["n"], r["batch"], r["direction"], r["bits"],
+                           arena_in[r["bits"]].data_ptr(), out_ptr(offset))
+            offset += nbytes
+            tickets.append(t)
+            inflight.append((t, nbytes))
+            used += nbytes
+        srv.drain()
+        makespan = time.perf_counter() - t0
+        for t, _ in inflight:
+            lat_of[t] = srv.wait(t)[1]
+        lat = [lat_of[t] for t in tickets]
+        stats = srv.stats()
+        srv.destroy()
+        return makespan, lat, stats
+
+    def summary(makespan, lat):
+        lat_ms = np.array(lat) * 1e3
+        return {"gflops": round(total_flops / makespan / 1e9, 1),
+                "p50_ms": round(float(np.percentile(lat_ms, 50)), 3),
+                "p99_ms": round(float(np.percentile(lat_ms, 99)), 3)}
+
+    zeros = [0.0] * len(reqs)
+    serial_span, serial_lat = run_serial(zeros)
+    srv_span, srv_lat, stats = run_server(zeros)
+    capacity = len(reqs) / serial_span           # serial requests per second
+    rates = {}
+    for frac in (0.5, 0.9):
+        rate = capacity * frac
+        rng = np.random.default_rng(5)
+        arrivals = list(np.cumsum(rng.exponential(1.0 / rate, size=len(reqs))))
+        s_span, s_lat = run_serial(arrivals)
+        v_span, v_lat, _ = run_server(arrivals)
+        rates[f"{rate:.0f}_req_per_s"] = {"serial": summary(s_span, s_lat),
+                                          "server": summary(v_span, v_lat)}
+    for p in plans.values():
+        p.destroy()
+    sat_server = summary(srv_span, srv_lat)
+    sat_serial = summary(serial_span, serial_lat)
+    return {
+        "metric": "serve C2C GFLOP/s (5n log2 n), saturation", "value": sat_server["gflops"],
+        "unit": "GFLOP/s", "n_gpus": world, "steps": 1, "warmup": 1,
+        "ms_per_step": round(srv_span * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": f"serving stream: first {len(reqs)} requests (seed 11) of the "
+                               "20,000-request stream: n Zipf(1.1) over 2^8..2^20, batch 1..256, "
+                               "80% FP32 / 20% FP64, device-resident payloads",
+                   "server": {"streams": 4, "hbm_budget_gib": 40}},
+        "saturation": {"server": sat_server, "serial_plain": sat_serial,
+                       "speedup": round(serial_span / srv_span, 2),
+                       "launches": stats["launches"], "requests": len(reqs)},
+        "poisson": rates,
+    }
+
+
 def main():
     args = parse_args()
     world, rank, local = dist_setup(args)
@@ -471,6 +690,16 @@ def main():
             return run_reference(args, world, rank)
         if args.sweep:
             run_sweep(args, world, rank, local)
+            return 0
+        if args.serve:
+            line = run_serve(args, world, rank, local)
+            if rank == 0:
+                print(json.dumps(line), flush=True)
+            return 0
+        if args.ragged:
+            line = run_ragged(args, world, rank, local)
+            if rank == 0:
+                print(json.dumps(line), flush=True)
             return 0
         line = run_gpu(args, world, rank, local)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:

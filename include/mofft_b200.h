@@ -71,6 +71,36 @@ mofft_status mofft_schedule_preview(int precision_bits, size_t length,
                                     mofft_plan_schedule *schedule,
                                     int *chain_out, size_t *chain_count);
 
+/* Ragged batches (no counterpart in the reference): many FP32 transforms of
+ * different lengths, batch sizes and directions executed by ONE persistent
+ * kernel launch over a work-descriptor queue, replayed from a CUDA graph.
+ * Items hold device buffers (input == output runs in place).  Supported
+ * lengths: 2^6 .. 2^13 and 3*2^5 .. 3*2^11 in one pass, and products of two
+ * column lengths in {96, 128, 192, 256} (e.g. 2^14 .. 2^16, 3*2^12, 3*2^13)
+ * in two passes; others give MOFFT_UNSUPPORTED_SIZE.
+ * mofft_ragged_execute enqueues the whole batch on `stream` (a
+ * cudaStream_t); mofft_ragged_status (blocking) reports whether the last
+ * execution completed every tile.  mofft_ragged_execute_per_item runs the
+ * same items as one ordinary batched plan each (the comparison point). */
+typedef struct mofft_ragged_plan mofft_ragged_plan;
+typedef struct {
+  size_t length;
+  size_t batch;
+  mofft_direction direction;
+  const void *input;   /* device, batch * length complex64, dense */
+  void *output;
+} mofft_ragged_item;
+mofft_status mofft_ragged_plan_create_f32(mofft_ragged_plan **plan,
+                                          const mofft_ragged_item *items,
+                                          size_t count);
+mofft_status mofft_ragged_execute(mofft_ragged_plan *plan, void *stream);
+mofft_status mofft_ragged_execute_per_item(mofft_ragged_plan *plan,
+                                           void *stream);
+mofft_status mofft_ragged_status(mofft_ragged_plan *plan);
+mofft_status mofft_ragged_plan_info(const mofft_ragged_plan *plan,
+                                    size_t *tiles, int *grid);
+void mofft_ragged_plan_destroy(mofft_ragged_plan *plan);
+
 /* Allocation-free execution (no counterpart in the reference).
  *
  * For callers that cannot allocate device memory: code embedded in a host
@@ -101,7 +131,39 @@ mofft_status mofft_execute_fixed_scratch_f32(const mofft_complex_f32 *input,
                                              mofft_direction direction,
                                              void *stream);
 
-/* Kernel registry introspection. */
+/* Precision forms of FP32 plans (no counterpart in the reference, whose
+ * transforms run in the plan's own precision on the CPU cores).
+ *
+ *   MOFFT_FORM_FP32    FP32 butterflies on the CUDA cores (the default).
+ *   MOFFT_FORM_TF32X3  the three radix-16 stages of n = 4096 as DFT-matrix
+ *                      GEMMs on the tensor cores; every operand x is split
+ *                      into TF32 terms hi + lo and each product is
+ *                      lo*hi + hi*lo + hi*hi, accumulated in FP32 (about 21
+ *                      significant bits per product).
+ *   MOFFT_FORM_BF16X3  the same with BF16 terms (about 16 bits).
+ *
+ * Tensor-core forms exist for FP32 plans of length 4096 only (other lengths:
+ * MOFFT_UNSUPPORTED_SIZE, the plan keeps its form); they run direct batches
+ * (not the serving engine's pointer tables).  Twiddle multiplications and
+ * the shuffles between stages stay FP32 on the CUDA cores.  The kernel bounds
+ * every wait on the tensor core: a wait that timed out makes the blocking
+ * execute return MOFFT_INTERNAL_ERROR; with an attached stream,
+ * mofft_plan_check_f32 (blocking) reports it.  Recipes record the FP32
+ * schedule; the form is not part of a recipe. */
+typedef enum {
+  MOFFT_FORM_FP32 = 0,
+  MOFFT_FORM_TF32X3 = 1,
+  MOFFT_FORM_BF16X3 = 2
+} mofft_precision_form;
+mofft_status mofft_plan_set_precision_form_f32(mofft_plan_f32 *plan,
+                                               mofft_precision_form form);
+mofft_status mofft_plan_get_precision_form_f32(const mofft_plan_f32 *plan,
+                                               mofft_precision_form *form);
+mofft_status mofft_plan_check_f32(mofft_plan_f32 *plan);
+
+/* Kernel registry introspection.  kind: 0 one-pass rows kernel, 1 column pass
+ * of a multi-pass transform, 2 generic (runtime radix list), 3 tensor-core
+ * precision form. */
 int mofft_kernel_count(void);
 /* Fills name (NUL-terminated, truncated to capacity) and shape of entry i;
  * returns 0 on success, -1 when i is out of range. */

@@ -39,6 +39,11 @@ OUT_OF_PLACE = 0
 IN_PLACE = 1
 PLANNER_PRETUNED = 0
 PLANNER_MEASURE = 1
+
+# precision forms of FP32 plans (mofft_precision_form)
+FORM_FP32 = 0
+FORM_TF32X3 = 1
+FORM_BF16X3 = 2
 PLAN_STRICT_WISDOM = 1
 FLAG_PRETUNED = 0
 FLAG_MEASURE = 1
@@ -48,7 +53,7 @@ STAGE_LAYOUT_SECTION = 1
 TRANSPOSE_LINEAR = 0
 TRANSPOSE_BLOCKED = 1
 MAX_PLAN_DEPTH = 64
-KERNEL_ROWS, KERNEL_COLS, KERNEL_GENERIC = 0, 1, 2
+KERNEL_ROWS, KERNEL_COLS, KERNEL_GENERIC, KERNEL_TENSOR = 0, 1, 2, 3
 
 
 class MofftError(RuntimeError):
@@ -95,6 +100,29 @@ class Schedule(ctypes.Structure):
     _fields_ = [("pass_count", ctypes.c_int), ("lengths", ctypes.c_int * 4),
                 ("kernels", ctypes.c_int * 4), ("smem_bytes", ctypes.c_size_t * 4),
                 ("workspace_bytes", ctypes.c_size_t), ("twiddle_bytes", ctypes.c_size_t)]
+
+
+class RaggedItem(ctypes.Structure):
+    _fields_ = [("length", ctypes.c_size_t), ("batch", ctypes.c_size_t),
+                ("direction", ctypes.c_int), ("input", ctypes.c_void_p),
+                ("output", ctypes.c_void_p)]
+
+
+class ServerOptions(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("streams", ctypes.c_int),
+                ("max_group_points", ctypes.c_size_t)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("length", ctypes.c_size_t), ("batch", ctypes.c_size_t),
+                ("direction", ctypes.c_int), ("precision_bits", ctypes.c_int),
+                ("input", ctypes.c_void_p), ("output", ctypes.c_void_p)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("failed", ctypes.c_uint64), ("launches", ctypes.c_uint64),
+                ("peak_admitted_bytes", ctypes.c_size_t)]
 
 
 _P = ctypes.c_void_p
@@ -154,6 +182,21 @@ _PLAIN = [
                                ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     ("mofft_launch_count", _U64, []),
     ("mofft_execute_fixed_scratch_f32", _I, [_P, _P, _SZ, _SZ, _I, _P]),
+    ("mofft_plan_set_precision_form_f32", _I, [_P, _I]),
+    ("mofft_plan_get_precision_form_f32", _I, [_P, ctypes.POINTER(_I)]),
+    ("mofft_plan_check_f32", _I, [_P]),
+    ("mofft_ragged_plan_create_f32", _I, [ctypes.POINTER(_P), ctypes.POINTER(RaggedItem), _SZ]),
+    ("mofft_ragged_execute", _I, [_P, _P]),
+    ("mofft_ragged_execute_per_item", _I, [_P, _P]),
+    ("mofft_ragged_status", _I, [_P]),
+    ("mofft_ragged_plan_info", _I, [_P, ctypes.POINTER(_SZ), ctypes.POINTER(_I)]),
+    ("mofft_ragged_plan_destroy", None, [_P]),
+    ("mofft_server_create", _I, [ctypes.POINTER(_P), ctypes.POINTER(ServerOptions)]),
+    ("mofft_server_submit", _I, [_P, ctypes.POINTER(Request), ctypes.POINTER(_U64)]),
+    ("mofft_server_wait", _I, [_P, _U64, ctypes.POINTER(ctypes.c_double)]),
+    ("mofft_server_drain", _I, [_P]),
+    ("mofft_server_get_stats", _I, [_P, ctypes.POINTER(ServerStats)]),
+    ("mofft_server_destroy", None, [_P]),
     ("mofft_schedule_preview", _I, [_I, _SZ, ctypes.POINTER(_I), _SZ, ctypes.c_uint,
                                     ctypes.POINTER(Schedule), ctypes.POINTER(_I),
                                     ctypes.POINTER(_SZ)]),
@@ -311,6 +354,26 @@ class Plan:
     def set_kernel_bank(self, bank: int) -> None:
         check(self._fn("plan_set_kernel_bank")(self._h, bank), "set_kernel_bank")
 
+    def set_precision_form(self, form: int) -> None:
+        """FP32 plans: FORM_FP32 (CUDA cores) or a tensor-core form."""
+        if self.bits != 32:
+            raise MofftError(1, "precision forms apply to FP32 plans")
+        check(self._lib.mofft_plan_set_precision_form_f32(self._h, form), "set_precision_form")
+
+    @property
+    def precision_form(self) -> int:
+        if self.bits != 32:
+            return FORM_FP32
+        v = ctypes.c_int()
+        check(self._lib.mofft_plan_get_precision_form_f32(self._h, ctypes.byref(v)),
+              "get_precision_form")
+        return v.value
+
+    def check_status(self) -> None:
+        """Blocking: raises if a tensor-core kernel of this plan recorded a timeout."""
+        if self.bits == 32:
+            check(self._lib.mofft_plan_check_f32(self._h), "check")
+
     def schedule(self) -> dict:
         s = Schedule()
         check(self._fn("plan_get_schedule")(self._h, ctypes.byref(s)), "schedule")
@@ -342,6 +405,96 @@ class Plan:
 
     def __exit__(self, *exc):
         self.destroy()
+
+
+class RaggedPlan:
+    """Many FP32 transforms of different lengths in one persistent launch.
+
+    `items` is a list of (input_tensor, output_tensor, direction) with
+    complex64 CUDA tensors of shape (batch, n); input is output for in place."""
+
+    def __init__(self, items):
+        self._lib = load()
+        arr = (RaggedItem * len(items))()
+        self._keep = []
+        for k, (x, y, direction) in enumerate(items):
+            n = x.shape[-1]
+            arr[k] = RaggedItem(n, x.numel() // n, direction, x.data_ptr(), y.data_ptr())
+            self._keep.append((x, y))
+        h = ctypes.c_void_p()
+        check(self._lib.mofft_ragged_plan_create_f32(ctypes.byref(h), arr, len(items)),
+              "ragged plan")
+        self._h = h
+
+    def execute(self, stream: Optional[int] = None) -> None:
+        check(self._lib.mofft_ragged_execute(self._h, stream), "ragged execute")
+
+    def execute_per_item(self, stream: Optional[int] = None) -> None:
+        check(self._lib.mofft_ragged_execute_per_item(self._h, stream), "per-item execute")
+
+    def status(self) -> int:
+        return self._lib.mofft_ragged_status(self._h)
+
+    def info(self) -> tuple[int, int]:
+        tiles = ctypes.c_size_t()
+        grid = ctypes.c_int()
+        check(self._lib.mofft_ragged_plan_info(self._h, ctypes.byref(tiles), ctypes.byref(grid)),
+              "ragged info")
+        return tiles.value, grid.value
+
+    def destroy(self) -> None:
+        if self._h and self._h.value:
+            self._lib.mofft_ragged_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching request engine (include/mofft_serve.h)."""
+
+    def __init__(self, hbm_budget_bytes: int = 0, streams: int = 0, max_group_points: int = 0):
+        self._lib = load()
+        h = ctypes.c_void_p()
+        opts = ServerOptions(hbm_budget_bytes, streams, max_group_points)
+        check(self._lib.mofft_server_create(ctypes.byref(h), ctypes.byref(opts)), "server")
+        self._h = h
+
+    def submit(self, length: int, batch: int, direction: int, bits: int, input_ptr: int,
+               output_ptr: int) -> int:
+        req = Request(length, batch, direction, bits, input_ptr, output_ptr)
+        ticket = ctypes.c_uint64()
+        check(self._lib.mofft_server_submit(self._h, ctypes.byref(req), ctypes.byref(ticket)),
+              "submit")
+        return ticket.value
+
+    def wait(self, ticket: int) -> tuple[int, float]:
+        lat = ctypes.c_double()
+        st = self._lib.mofft_server_wait(self._h, ticket, ctypes.byref(lat))
+        return st, lat.value
+
+    def drain(self) -> None:
+        check(self._lib.mofft_server_drain(self._h), "drain")
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        check(self._lib.mofft_server_get_stats(self._h, ctypes.byref(s)), "stats")
+        return {f: getattr(s, f) for f, _ in ServerStats._fields_}
+
+    def destroy(self) -> None:
+        if self._h and self._h.value:
+            self._lib.mofft_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
 
 
 def fft(x, direction: int = FORWARD, *, inplace: bool = False):

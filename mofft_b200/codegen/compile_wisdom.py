@@ -6,10 +6,12 @@ Input: ``mofft_b200/wisdom/b200_wisdom.json``::
 
     {"source": "...", "formal": false,
      "entries": [{"length": 4096, "precision_bits": 32,
-                  "chain": [16, 16, 16]}, ...]}
+                  "chain": [16, 16, 16],
+                  "kernels": ["rows_float_4096_t256_b1_sfalse"]}, ...]}
 
 ``chain`` is the in-CTA Stockham stage list, first stage first (the
-reference's radix chain reversed).  Entries are validated: the chain must
+reference's radix chain reversed); ``kernels`` (optional) names the tuned
+kernel instance of each pass among the variants that share a chain.  Entries are validated: the chain must
 multiply to the length and use only radices of the reference's set.
 
 Run: python -m mofft_b200.codegen.compile_wisdom [json] [out_header]
@@ -47,7 +49,8 @@ def load_entries(path: Path) -> tuple[list[dict], str, bool]:
         if key in seen:
             raise ValueError(f"duplicate wisdom entry {key}")
         seen.add(key)
-        entries.append({"length": length, "bits": bits, "chain": chain})
+        kernels = [str(k) for k in e.get("kernels", [])][:4]
+        entries.append({"length": length, "bits": bits, "chain": chain, "kernels": kernels})
     entries.sort(key=lambda e: (e["bits"], e["length"]))
     return entries, str(data.get("source", "unknown")), bool(data.get("formal", False))
 
@@ -57,13 +60,16 @@ def render(entries: list[dict], source: str, formal: bool) -> str:
         "/* Generated by mofft_b200/codegen/compile_wisdom.py -- do not edit. */",
         "#pragma once",
         "#include <stddef.h>",
-        "typedef struct { size_t length; int precision_bits; int count; int chain[24]; } mofft_wisdom_entry;",
+        "typedef struct { size_t length; int precision_bits; int count; int chain[24];"
+        " const char *kernels[4]; } mofft_wisdom_entry;",
         "static const mofft_wisdom_entry k_mofft_wisdom[] = {",
     ]
     for e in entries:
         chain = ", ".join(str(r) for r in e["chain"])
-        lines.append(f"  {{{e['length']}u, {e['bits']}, {len(e['chain'])}, {{{chain}}}}},")
-    lines.append("  {0u, 0, 0, {0}},")
+        names = ", ".join(f'"{k}"' for k in e["kernels"]) or "0"
+        lines.append(f"  {{{e['length']}u, {e['bits']}, {len(e['chain'])}, {{{chain}}}, "
+                     f"{{{names}}}}},")
+    lines.append("  {0u, 0, 0, {0}, {0}},")
     lines.append("};")
     lines.append(f"#define MOFFT_WISDOM_COUNT {len(entries)}")
     lines.append(f"#define MOFFT_WISDOM_FORMAL {1 if formal else 0}")

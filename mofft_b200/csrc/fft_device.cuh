@@ -164,8 +164,38 @@ struct ColsLayout {
   }
 };
 
+// Kernel flags (template parameter FLAGS of the ROWS kernels).
+constexpr int kStaged = 1;       // I/O staged through shared memory
+constexpr int kDerivedTw = 2;    // radix-16 twiddles from w, w^2, w^4, w^8
+
+// Twiddles of one radix-16 butterfly: v[r] *= w^r.  Loads the table entries
+// of w^1, w^2, w^4 and w^8 and forms the other powers with at most three
+// chained complex products (three roundings), instead of 15 table loads.
+template <typename T, int NS, int TWOFF>
+__device__ __forceinline__ void twiddle16_derived(T (&vr)[16], T (&vi)[16], int jm,
+                                                  const cplx_t<T>* __restrict__ tw) {
+  T wr[16], wi[16];
+  const cplx_t<T> a1 = __ldg(tw + TWOFF + 0 * NS + jm);
+  const cplx_t<T> a2 = __ldg(tw + TWOFF + 1 * NS + jm);
+  const cplx_t<T> a4 = __ldg(tw + TWOFF + 3 * NS + jm);
+  const cplx_t<T> a8 = __ldg(tw + TWOFF + 7 * NS + jm);
+  wr[1] = a1.x; wi[1] = a1.y;
+  wr[2] = a2.x; wi[2] = a2.y;
+  wr[4] = a4.x; wi[4] = a4.y;
+  wr[8] = a8.x; wi[8] = a8.y;
+#define MOFFT_WMUL(D, A, B)                          \
+  wr[D] = wr[A] * wr[B] - wi[A] * wi[B];             \
+  wi[D] = wr[A] * wi[B] + wi[A] * wr[B];
+  MOFFT_WMUL(3, 2, 1) MOFFT_WMUL(5, 4, 1) MOFFT_WMUL(6, 4, 2) MOFFT_WMUL(7, 4, 3)
+  MOFFT_WMUL(9, 8, 1) MOFFT_WMUL(10, 8, 2) MOFFT_WMUL(11, 8, 3) MOFFT_WMUL(12, 8, 4)
+  MOFFT_WMUL(13, 8, 5) MOFFT_WMUL(14, 8, 6) MOFFT_WMUL(15, 8, 7)
+#undef MOFFT_WMUL
+#pragma unroll
+  for (int r = 1; r < 16; ++r) cmul<T>(vr[r], vi[r], wr[r], wi[r]);
+}
+
 template <typename T, int L, int TPL, int R, int NS, Where SRC, Where DST,
-          int TWOFF, class Layout>
+          int TWOFF, bool DTW, class Layout>
 __device__ __forceinline__ void reg_stage(const Layout& lay, int t,
                                           const cplx_t<T>* __restrict__ tw) {
   constexpr int BF = L / R;
@@ -189,10 +219,14 @@ __device__ __forceinline__ void reg_stage(const Layout& lay, int t,
       }
       if (NS > 1) {
         const int jm = j % NS;
+        if constexpr (DTW && R == 16) {
+          twiddle16_derived<T, NS, TWOFF>(vr[m], vi[m], jm, tw);
+        } else {
 #pragma unroll
-        for (int r = 1; r < R; ++r) {
-          const cplx_t<T> w = __ldg(tw + TWOFF + (r - 1) * NS + jm);
-          cmul<T>(vr[m][r], vi[m][r], w.x, w.y);
+          for (int r = 1; r < R; ++r) {
+            const cplx_t<T> w = __ldg(tw + TWOFF + (r - 1) * NS + jm);
+            cmul<T>(vr[m][r], vi[m][r], w.x, w.y);
+          }
         }
       }
       Dft<R>::fwd(vr[m], vi[m]);
@@ -221,31 +255,31 @@ __device__ __forceinline__ void reg_stage(const Layout& lay, int t,
 
 // Recursive stage driver over a compile-time radix list.
 template <typename T, int L, int TPL, int NS, int TWOFF, bool FIRST_SHARED,
-          bool LAST_SHARED, bool IS_FIRST, int... Rs>
+          bool LAST_SHARED, bool IS_FIRST, bool DTW, int... Rs>
 struct StageRunner;
 
 template <typename T, int L, int TPL, int NS, int TWOFF, bool FS, bool LS,
-          bool IS_FIRST, int R>
-struct StageRunner<T, L, TPL, NS, TWOFF, FS, LS, IS_FIRST, R> {
+          bool IS_FIRST, bool DTW, int R>
+struct StageRunner<T, L, TPL, NS, TWOFF, FS, LS, IS_FIRST, DTW, R> {
   template <class Layout>
   __device__ __forceinline__ static void run(const Layout& lay, int t,
                                              const cplx_t<T>* tw) {
     constexpr Where src = (IS_FIRST && !FS) ? kGlobal : kShared;
     constexpr Where dst = LS ? kShared : kGlobal;
-    reg_stage<T, L, TPL, R, NS, src, dst, TWOFF>(lay, t, tw);
+    reg_stage<T, L, TPL, R, NS, src, dst, TWOFF, DTW>(lay, t, tw);
   }
 };
 
 template <typename T, int L, int TPL, int NS, int TWOFF, bool FS, bool LS,
-          bool IS_FIRST, int R, int R2, int... Rest>
-struct StageRunner<T, L, TPL, NS, TWOFF, FS, LS, IS_FIRST, R, R2, Rest...> {
+          bool IS_FIRST, bool DTW, int R, int R2, int... Rest>
+struct StageRunner<T, L, TPL, NS, TWOFF, FS, LS, IS_FIRST, DTW, R, R2, Rest...> {
   template <class Layout>
   __device__ __forceinline__ static void run(const Layout& lay, int t,
                                              const cplx_t<T>* tw) {
     constexpr Where src = (IS_FIRST && !FS) ? kGlobal : kShared;
-    reg_stage<T, L, TPL, R, NS, src, kShared, TWOFF>(lay, t, tw);
+    reg_stage<T, L, TPL, R, NS, src, kShared, TWOFF, DTW>(lay, t, tw);
     StageRunner<T, L, TPL, NS * R, TWOFF + stage_table_size(R, NS), FS, LS,
-                false, R2, Rest...>::run(lay, t, tw);
+                false, DTW, R2, Rest...>::run(lay, t, tw);
   }
 };
 
@@ -264,14 +298,33 @@ struct RowsArgs {
   long long in_dist;
   long long out_dist;
   T sign;
+  // Indirect batch (may be null): transform b reads in_table[b] and writes
+  // out_table[b] instead of in + b*in_dist / out + b*out_dist.  This lets one
+  // launch serve transforms that live in unrelated buffers.
+  const cplx_t<T>* const* in_table;
+  cplx_t<T>* const* out_table;
 };
+
+template <typename T>
+__device__ __forceinline__ const cplx_t<T>* batch_in(const cplx_t<T>* base, long long dist,
+                                                     const cplx_t<T>* const* table,
+                                                     long long b) {
+  return table ? table[b] : base + b * dist;
+}
+template <typename T>
+__device__ __forceinline__ cplx_t<T>* batch_out(cplx_t<T>* base, long long dist,
+                                                cplx_t<T>* const* table, long long b) {
+  return table ? table[b] : base + b * dist;
+}
 
 // Body of one ROWS tile: transforms b0 .. b0+TB-1, run by threads
 // 0 .. TPL*TB-1 of the CTA (every thread of the CTA must call it).
-template <typename T, int L, int TPL, int TB, bool STAGED, int... Rs>
+template <typename T, int L, int TPL, int TB, int FLAGS, int... Rs>
 __device__ __forceinline__ void rows_body(const RowsArgs<T>& a, long long b0,
                                           unsigned char* smem_raw) {
   static_assert(StageProduct<L, Rs...>::value == L, "radices must multiply to L");
+  constexpr bool STAGED = (FLAGS & kStaged) != 0;
+  constexpr bool DTW = (FLAGS & kDerivedTw) != 0;
   constexpr int LINE = spad_len<T>(L);
   T* sre = reinterpret_cast<T*>(smem_raw);
   T* sim = sre + TB * LINE;
@@ -281,10 +334,10 @@ __device__ __forceinline__ void rows_body(const RowsArgs<T>& a, long long b0,
   RowsLayout<T> lay;
   lay.sre = sre + line * LINE;
   lay.sim = sim + line * LINE;
-  lay.gin = a.in + b * a.in_dist;
-  lay.gout = a.out + b * a.out_dist;
-  lay.sign = a.sign;
   lay.active = b < a.batch;
+  lay.gin = lay.active ? batch_in<T>(a.in, a.in_dist, a.in_table, b) : a.in;
+  lay.gout = lay.active ? batch_out<T>(a.out, a.out_dist, a.out_table, b) : a.out;
+  lay.sign = a.sign;
   if (STAGED) {
     // Cooperative load of lines b0 .. b0+TB-1 (each L contiguous elements).
     const long long lines = (a.batch - b0) < TB ? (a.batch - b0) : TB;
@@ -292,32 +345,33 @@ __device__ __forceinline__ void rows_body(const RowsArgs<T>& a, long long b0,
       const int ln = q / L;
       const int i = q - ln * L;
       if (ln < lines) {
-        const cplx_t<T> v = ld_global<T>(a.in + (b0 + ln) * a.in_dist + i);
+        const cplx_t<T> v =
+            ld_global<T>(batch_in<T>(a.in, a.in_dist, a.in_table, b0 + ln) + i);
         sre[ln * LINE + spad<T>(i)] = v.x;
         sim[ln * LINE + spad<T>(i)] = v.y * a.sign;
       }
     }
     __syncthreads();
   }
-  StageRunner<T, L, TPL, 1, 0, STAGED, STAGED, true, Rs...>::run(lay, t, a.tw);
+  StageRunner<T, L, TPL, 1, 0, STAGED, STAGED, true, DTW, Rs...>::run(lay, t, a.tw);
   if (STAGED) {
     const long long lines = (a.batch - b0) < TB ? (a.batch - b0) : TB;
     for (int q = threadIdx.x; q < TB * L; q += TPL * TB) {
       const int ln = q / L;
       const int i = q - ln * L;
       if (ln < lines)
-        st_global<T>(a.out + (b0 + ln) * a.out_dist + i,
+        st_global<T>(batch_out<T>(a.out, a.out_dist, a.out_table, b0 + ln) + i,
                      sre[ln * LINE + spad<T>(i)],
                      sim[ln * LINE + spad<T>(i)] * a.sign);
     }
   }
 }
 
-template <typename T, int L, int TPL, int TB, bool STAGED, int... Rs>
+template <typename T, int L, int TPL, int TB, int FLAGS, int... Rs>
 __global__ void __launch_bounds__(TPL * TB)
 rows_kernel(const RowsArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  rows_body<T, L, TPL, TB, STAGED, Rs...>(a, (long long)blockIdx.x * TB, smem_raw);
+  rows_body<T, L, TPL, TB, FLAGS, Rs...>(a, (long long)blockIdx.x * TB, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -343,6 +397,8 @@ struct ColsArgs {
   int split_shift;
   T sign_in;
   T sign_out;
+  const cplx_t<T>* const* in_table;   // indirect batch, may be null
+  cplx_t<T>* const* out_table;
 };
 
 template <typename T, int L, int TPL, int C>
@@ -373,9 +429,11 @@ __device__ __forceinline__ void cols_body(const ColsArgs<T>& a, long long b,
   lay.sre = sre;
   lay.sim = sim;
   lay.c = c;
-  lay.gin = a.in + b * a.in_dist + j;
+  const cplx_t<T>* in_b = batch_in<T>(a.in, a.in_dist, a.in_table, b);
+  cplx_t<T>* out_b = batch_out<T>(a.out, a.out_dist, a.out_table, b);
+  lay.gin = in_b + j;
   lay.in_stride = lines_total;
-  lay.gout = a.out + b * a.out_dist + jq * ns * L + jm;
+  lay.gout = out_b + jq * ns * L + jm;
   lay.out_stride = ns;
   lay.sign_in = a.sign_in;
   lay.sign_out = a.sign_out;
@@ -385,9 +443,9 @@ __device__ __forceinline__ void cols_body(const ColsArgs<T>& a, long long b,
   lay.jmod = jm;
   lay.split_shift = a.split_shift;
   if (ns == 1) {
-    StageRunner<T, L, TPL, 1, 0, false, true, true, Rs...>::run(lay, t, a.tw);
+    StageRunner<T, L, TPL, 1, 0, false, true, true, false, Rs...>::run(lay, t, a.tw);
     // lines j0..j0+C-1 are contiguous: out[b*dist + j0*L + c*L + k]
-    cplx_t<T>* dst = a.out + b * a.out_dist + j0 * L;
+    cplx_t<T>* dst = out_b + j0 * L;
     if (lay.active) {
       for (int q = threadIdx.x; q < C * L; q += G::THREADS) {
         const int cc = q / L;
@@ -397,7 +455,7 @@ __device__ __forceinline__ void cols_body(const ColsArgs<T>& a, long long b,
       }
     }
   } else {
-    StageRunner<T, L, TPL, 1, 0, false, false, true, Rs...>::run(lay, t, a.tw);
+    StageRunner<T, L, TPL, 1, 0, false, false, true, false, Rs...>::run(lay, t, a.tw);
   }
 }
 

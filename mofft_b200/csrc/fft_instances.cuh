@@ -26,6 +26,8 @@ RowsArgs<T> rows_args(const mofft_pass_args *p) {
   a.in_dist = p->in_dist;
   a.out_dist = p->out_dist;
   a.sign = p->conj_in ? T(-1) : T(1);
+  a.in_table = reinterpret_cast<const cplx_t<T> *const *>(p->in_table);
+  a.out_table = reinterpret_cast<cplx_t<T> *const *>(p->out_table);
   return a;
 }
 
@@ -45,35 +47,37 @@ ColsArgs<T> cols_args(const mofft_pass_args *p) {
   a.split_shift = p->split_shift;
   a.sign_in = p->conj_in ? T(-1) : T(1);
   a.sign_out = p->conj_out ? T(-1) : T(1);
+  a.in_table = reinterpret_cast<const cplx_t<T> *const *>(p->in_table);
+  a.out_table = reinterpret_cast<cplx_t<T> *const *>(p->out_table);
   return a;
 }
 
-template <typename T, int L, int TPL, int TB, bool STAGED, int... Rs>
+template <typename T, int L, int TPL, int TB, int FLAGS, int... Rs>
 struct RowsInst {
   static constexpr size_t smem() {
     return 2ull * TB * spad_len<T>(L) * sizeof(T);
   }
   static const void *func() {
-    return reinterpret_cast<const void *>(&rows_kernel<T, L, TPL, TB, STAGED, Rs...>);
+    return reinterpret_cast<const void *>(&rows_kernel<T, L, TPL, TB, FLAGS, Rs...>);
   }
   static cudaError_t launch(const mofft_pass_args *p, cudaStream_t s) {
     if (p->conj_in != p->conj_out) return cudaErrorInvalidValue;
     const long long grid = (p->batch + TB - 1) / TB;
     if (grid <= 0) return cudaSuccess;
     if (grid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-    rows_kernel<T, L, TPL, TB, STAGED, Rs...>
+    rows_kernel<T, L, TPL, TB, FLAGS, Rs...>
         <<<(unsigned)grid, TPL * TB, smem(), s>>>(rows_args<T>(p));
     return cudaGetLastError();
   }
   static Entry entry(const char *name) {
-    Entry e;
+    Entry e{};
     e.desc.name = name;
     e.desc.precision_bits = sizeof(T) == 4 ? 32 : 64;
     e.desc.kind = MOFFT_KERNEL_ROWS;
     e.desc.length = L;
     e.desc.lines = TB;
     e.desc.threads = TPL * TB;
-    e.desc.staged = STAGED ? 1 : 0;
+    e.desc.staged = (FLAGS & kStaged) ? 1 : 0;
     const int rs[] = {Rs...};
     e.desc.radix_count = (int)sizeof...(Rs);
     for (int i = 0; i < 8; ++i) e.desc.radices[i] = i < (int)sizeof...(Rs) ? rs[i] : 0;
@@ -102,7 +106,7 @@ struct ColsInst {
     return cudaGetLastError();
   }
   static Entry entry(const char *name) {
-    Entry e;
+    Entry e{};
     e.desc.name = name;
     e.desc.precision_bits = sizeof(T) == 4 ? 32 : 64;
     e.desc.kind = MOFFT_KERNEL_COLS;
@@ -150,6 +154,7 @@ struct GenericInst {
     a.stage_count = p->radix_count;
     if (p->radix_count < 1 || p->radix_count > kMaxGenericStages || p->lines < 1)
       return cudaErrorInvalidValue;
+    if (p->in_table || p->out_table) return cudaErrorNotSupported;
     long long prod = 1;
     for (int i = 0; i < kMaxGenericStages; ++i) {
       a.radices[i] = i < p->radix_count ? p->radices[i] : 0;
@@ -176,7 +181,7 @@ struct GenericInst {
     return cudaGetLastError();
   }
   static Entry entry(const char *name) {
-    Entry e;
+    Entry e{};
     e.desc.name = name;
     e.desc.precision_bits = sizeof(T) == 4 ? 32 : 64;
     e.desc.kind = MOFFT_KERNEL_GENERIC;
@@ -196,8 +201,14 @@ struct GenericInst {
 };
 
 
+// ST: true/false (staged I/O); ROWSD: staged flag plus derived radix-16
+// twiddles (name suffix _d).
 #define ROWS(T, L, TPL, TB, ST, ...) \
-  RowsInst<T, L, TPL, TB, ST, __VA_ARGS__>::entry("rows_" #T "_" #L "_t" #TPL "_b" #TB "_s" #ST)
+  RowsInst<T, L, TPL, TB, (ST) ? kStaged : 0, __VA_ARGS__>::entry( \
+      "rows_" #T "_" #L "_t" #TPL "_b" #TB "_s" #ST)
+#define ROWSD(T, L, TPL, TB, ST, ...) \
+  RowsInst<T, L, TPL, TB, ((ST) ? kStaged : 0) | kDerivedTw, __VA_ARGS__>::entry( \
+      "rows_" #T "_" #L "_t" #TPL "_b" #TB "_s" #ST "_d")
 #define COLS(T, L, TPL, C, ...) \
   ColsInst<T, L, TPL, C, __VA_ARGS__>::entry("cols_" #T "_" #L "_t" #TPL "_c" #C)
 
@@ -209,5 +220,6 @@ const Entry *entries_cols_f32(int *count);
 const Entry *entries_cols_f64(int *count);
 const Entry *entries_rows_mixed(int *count);
 const Entry *entries_cols_mixed(int *count);
+const Entry *entries_tensor(int *count);
 
 }  // namespace mofft

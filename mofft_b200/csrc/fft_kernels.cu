@@ -16,7 +16,7 @@ const std::vector<Entry> &registry() {
     const Entry *(*lists[])(int *) = {entries_generic, entries_rows_f32,
                                       entries_rows_f64, entries_cols_f32,
                                       entries_cols_f64, entries_rows_mixed,
-                                      entries_cols_mixed};
+                                      entries_cols_mixed, entries_tensor};
     for (auto list : lists) {
       int n = 0;
       const Entry *e = list(&n);

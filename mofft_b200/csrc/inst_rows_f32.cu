@@ -24,6 +24,15 @@ const Entry *entries_rows_f32(int *count) {
       ROWS(float, 4096, 512, 1, false, 16, 16, 16),
       ROWS(float, 8192, 512, 1, false, 16, 16, 16, 2),
       ROWS(float, 16384, 512, 1, false, 16, 16, 16, 4),
+      // derived radix-16 twiddles (fewer table loads through L1)
+      ROWSD(float, 256, 16, 16, true, 16, 16),
+      ROWSD(float, 512, 32, 8, false, 16, 16, 2),
+      ROWSD(float, 1024, 64, 4, false, 16, 16, 4),
+      ROWSD(float, 2048, 128, 2, false, 16, 16, 8),
+      ROWSD(float, 4096, 256, 1, false, 16, 16, 16),
+      ROWSD(float, 4096, 512, 1, false, 16, 16, 16),
+      ROWSD(float, 8192, 512, 1, false, 16, 16, 16, 2),
+      ROWSD(float, 16384, 512, 1, false, 16, 16, 16, 4),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;

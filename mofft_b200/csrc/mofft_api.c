@@ -299,9 +299,22 @@ static int score_less(const group_score *a, const group_score *b) {
 
 /* Fill one pass for stages [begin, end) of `chain`.  Returns 1 if some kernel
  * can run it (specialised when allowed, else generic). */
+static int kernel_fits(int k, int precision_bits, int kind, const int *chain,
+                       int count, long long total, long long ns_outer) {
+  const mofft_kernel_desc *d = mofft_cuda_kernel_get(k);
+  if (!d || d->kind != kind || d->precision_bits != precision_bits ||
+      !chain_equal(d->radices, d->radix_count, chain, count))
+    return 0;
+  if (kind == MOFFT_KERNEL_COLS) {
+    if ((total / d->length) % d->lines != 0) return 0;
+    if (ns_outer != 1 && ns_outer % d->lines != 0) return 0;
+  }
+  return 1;
+}
+
 static int make_pass(int precision_bits, unsigned bank, const int *chain,
                      int begin, int end, long long total, long long ns_outer,
-                     int single, mofft_pass *out) {
+                     int single, const int *preferred, mofft_pass *out) {
   const int count = end - begin;
   if (count < 1 || count > MOFFT_CUDA_MAX_STAGES) return 0;
   long long length = 1;
@@ -314,8 +327,14 @@ static int make_pass(int precision_bits, unsigned bank, const int *chain,
   out->ns_outer = ns_outer;
   const int kind = single ? MOFFT_KERNEL_ROWS : MOFFT_KERNEL_COLS;
   if (bank == 0 && count <= 8) {
-    const int k = find_special(precision_bits, kind, chain + begin, count,
-                               total, ns_outer);
+    int k = -1;
+    for (int i = 0; preferred && i < MOFFT_MAX_PASSES && k < 0; ++i)
+      if (preferred[i] >= 0 &&
+          kernel_fits(preferred[i], precision_bits, kind, chain + begin, count, total,
+                      ns_outer))
+        k = preferred[i];
+    if (k < 0)
+      k = find_special(precision_bits, kind, chain + begin, count, total, ns_outer);
     if (k >= 0) {
       const mofft_kernel_desc *d = mofft_cuda_kernel_get(k);
       out->kernel = k;
@@ -342,7 +361,8 @@ static int make_pass(int precision_bits, unsigned bank, const int *chain,
 /* Evaluate the split of `chain` at the given boundaries. */
 static int try_split(int precision_bits, unsigned bank, const int *chain,
                      int count, const int *cuts, int passes, long long total,
-                     mofft_schedule *sched, group_score *score) {
+                     const int *preferred, mofft_schedule *sched,
+                     group_score *score) {
   long long ns = 1;
   double lo = 1e300, hi = 0;
   int generic = 0;
@@ -350,7 +370,7 @@ static int try_split(int precision_bits, unsigned bank, const int *chain,
     const int begin = p == 0 ? 0 : cuts[p - 1];
     const int end = p == passes - 1 ? count : cuts[p];
     if (!make_pass(precision_bits, bank, chain, begin, end, total, ns,
-                   passes == 1, &sched->pass[p]))
+                   passes == 1, preferred, &sched->pass[p]))
       return 0;
     if (sched->pass[p].kind == MOFFT_KERNEL_GENERIC) ++generic;
     const double l = log2((double)sched->pass[p].length);
@@ -366,8 +386,9 @@ static int try_split(int precision_bits, unsigned bank, const int *chain,
 }
 
 /* Canonical grouping of a Stockham stage chain into passes. */
-int mofft_group_chain(int precision_bits, unsigned bank, const int *chain,
-                      int count, long long total, mofft_schedule *best) {
+int mofft_group_chain_preferred(int precision_bits, unsigned bank,
+                                const int *chain, int count, long long total,
+                                const int *preferred, mofft_schedule *best) {
   group_score best_score = {1 << 30, 1 << 30, 1e300};
   int found = 0;
   mofft_schedule cand;
@@ -378,7 +399,7 @@ int mofft_group_chain(int precision_bits, unsigned bank, const int *chain,
     for (int i = 0; i < passes - 1; ++i) cuts[i] = i + 1;
     for (;;) {
       if (try_split(precision_bits, bank, chain, count, cuts, passes, total,
-                    &cand, &score) &&
+                    preferred, &cand, &score) &&
           (!found || score_less(&score, &best_score))) {
         *best = cand;
         best_score = score;
@@ -394,6 +415,12 @@ int mofft_group_chain(int precision_bits, unsigned bank, const int *chain,
     if (found) break;
   }
   return found;
+}
+
+int mofft_group_chain(int precision_bits, unsigned bank, const int *chain,
+                      int count, long long total, mofft_schedule *best) {
+  return mofft_group_chain_preferred(precision_bits, bank, chain, count, total,
+                                     NULL, best);
 }
 
 /* Default in-CTA radix chain for a runtime-stage (generic) line of length L. */
@@ -502,7 +529,7 @@ int mofft_model_chain(int precision_bits, unsigned bank, size_t length,
         if (!ok) continue;
         group_score score;
         if (!try_split(precision_bits, bank, tmp, total_count, cuts, passes, n,
-                       &sched, &score))
+                       NULL, &sched, &score))
           continue;
         if (best_count < 0 || score_less(&score, &best)) {
           best = score;
@@ -563,6 +590,13 @@ static mofft_status materialise_schedule(mofft_core *c) {
       ps->tw_lo_offset = bytes;
       bytes = align256(bytes + lo_n * cb);
     }
+    ps->aux_offset = ps->status_offset = 0;
+    if (ps->kind == MOFFT_KERNEL_TENSOR) {
+      ps->aux_offset = bytes;
+      bytes = align256(bytes + mofft_cuda_tensor_aux_bytes(mofft_cuda_kernel_get(ps->kernel)->form));
+      ps->status_offset = bytes;
+      bytes = align256(bytes + sizeof(int));
+    }
   }
   if (bytes == 0) bytes = 256;
   unsigned char *host = (unsigned char *)calloc(1, bytes);
@@ -578,6 +612,21 @@ static mofft_status materialise_schedule(mofft_core *c) {
       mofft_write_twiddles(host + ps->tw_hi_offset, c->precision_bits, m, 0, lo_n, hi_n);
       mofft_write_twiddles(host + ps->tw_lo_offset, c->precision_bits, m, 0, 1, lo_n);
     }
+    if (ps->kind == MOFFT_KERNEL_TENSOR) {
+      double fr[256], fi[256];
+      for (int k = 0; k < 16; ++k)
+        for (int r = 0; r < 16; ++r) {
+          long double cr, si;
+          mofft_cis_turns((uint64_t)((k * r) % 16), 16, &cr, &si);
+          fr[k * 16 + r] = (double)cr;
+          fi[k * 16 + r] = -(double)si; /* forward sign */
+        }
+      if (mofft_cuda_tensor_fill_aux(mofft_cuda_kernel_get(ps->kernel)->form,
+                                     host + ps->aux_offset, fr, fi) != 0) {
+        free(host);
+        return MOFFT_INTERNAL_ERROR;
+      }
+    }
   }
   release_device(c);
   if (cudaMalloc(&c->d_twiddles, bytes) != cudaSuccess) {
@@ -586,8 +635,12 @@ static mofft_status materialise_schedule(mofft_core *c) {
     return MOFFT_ALLOCATION_FAILURE;
   }
   c->twiddle_bytes = bytes;
-  if (cudaMemcpy(c->d_twiddles, host, bytes, cudaMemcpyHostToDevice) !=
-      cudaSuccess) {
+  /* A cudaMemcpy from pageable memory may return before its DMA has landed,
+   * and plans run on non-blocking streams: copy on the plan's stream and
+   * wait for it, so the tables are complete before any later launch. */
+  if (cudaMemcpyAsync(c->d_twiddles, host, bytes, cudaMemcpyHostToDevice,
+                      (cudaStream_t)c->stream) != cudaSuccess ||
+      cudaStreamSynchronize((cudaStream_t)c->stream) != cudaSuccess) {
     cudaGetLastError();
     free(host);
     return MOFFT_INTERNAL_ERROR;
@@ -618,12 +671,60 @@ static int chain_from_factors(const mofft_core *c, int *chain) {
 }
 
 /* (Re)build the GPU schedule from c->factors and c->kernel_bank. */
+static int tensor_kernel_index(int form) {
+  const int n = mofft_cuda_kernel_count();
+  for (int i = 0; i < n; ++i) {
+    const mofft_kernel_desc *d = mofft_cuda_kernel_get(i);
+    if (d->kind == MOFFT_KERNEL_TENSOR && d->form == form) return i;
+  }
+  return -1;
+}
+
+/* One-pass schedule of the tensor-core kernel of c->form. */
+static mofft_status build_tensor_schedule(mofft_core *c) {
+  const int k = tensor_kernel_index(c->form);
+  if (k < 0) return MOFFT_UNSUPPORTED_SIZE;
+  const mofft_kernel_desc *d = mofft_cuda_kernel_get(k);
+  if (c->precision_bits != d->precision_bits || c->length != (size_t)d->length)
+    return MOFFT_UNSUPPORTED_SIZE;
+  mofft_schedule sched;
+  memset(&sched, 0, sizeof(sched));
+  sched.pass_count = 1;
+  mofft_pass *ps = &sched.pass[0];
+  ps->kernel = k;
+  ps->kind = MOFFT_KERNEL_TENSOR;
+  ps->length = d->length;
+  ps->lines = d->lines;
+  ps->radix_count = d->radix_count;
+  memcpy(ps->radices, d->radices, (size_t)d->radix_count * sizeof(int));
+  ps->ns_outer = 1;
+  ps->smem_bytes = d->smem_bytes;
+  c->sched = sched;
+  return materialise_schedule(c);
+}
+
+mofft_status mofft_core_check_status(const mofft_core *c) {
+  for (int p = 0; p < c->sched.pass_count; ++p) {
+    const mofft_pass *ps = &c->sched.pass[p];
+    if (ps->kind != MOFFT_KERNEL_TENSOR) continue;
+    int word = 0;
+    if (cudaMemcpy(&word, (const unsigned char *)c->d_twiddles + ps->status_offset,
+                   sizeof(word), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      cudaGetLastError();
+      return MOFFT_INTERNAL_ERROR;
+    }
+    if (word != 0) return MOFFT_INTERNAL_ERROR;
+  }
+  return MOFFT_SUCCESS;
+}
+
 mofft_status mofft_core_build(mofft_core *c) {
+  if (c->form != 0) return build_tensor_schedule(c);
   int chain[MOFFT_MAX_STAGES];
   const int count = chain_from_factors(c, chain);
   mofft_schedule sched;
-  if (!mofft_group_chain(c->precision_bits, c->kernel_bank, chain, count,
-                         (long long)c->length, &sched))
+  if (!mofft_group_chain_preferred(c->precision_bits, c->kernel_bank, chain, count,
+                                   (long long)c->length, c->preferred, &sched))
     return MOFFT_UNSUPPORTED_SIZE;
   c->sched = sched;
   return materialise_schedule(c);
@@ -635,6 +736,15 @@ mofft_status mofft_core_create(mofft_core **out, int precision_bits,
                                mofft_direction direction,
                                mofft_placement placement, const int *chain,
                                int chain_count) {
+  return mofft_core_create_tuned(out, precision_bits, length, batch, distance,
+                                 direction, placement, chain, chain_count, NULL);
+}
+
+mofft_status mofft_core_create_tuned(mofft_core **out, int precision_bits,
+                                     size_t length, size_t batch,
+                                     size_t distance, mofft_direction direction,
+                                     mofft_placement placement, const int *chain,
+                                     int chain_count, const int *preferred) {
   *out = NULL;
   if (!mofft_hardware_supports(precision_bits)) return MOFFT_UNSUPPORTED_HARDWARE;
   if (length < 2 || length > ((size_t)1 << 34)) return MOFFT_UNSUPPORTED_SIZE;
@@ -655,6 +765,8 @@ mofft_status mofft_core_create(mofft_core **out, int precision_bits,
   c->distance = distance;
   c->direct_input = 1;
   c->stage_layout = MOFFT_STAGE_LAYOUT_TRANSPOSE;
+  for (int i = 0; i < MOFFT_MAX_PASSES; ++i)
+    c->preferred[i] = preferred ? preferred[i] : -1;
   cudaGetDevice(&c->device);
   int tmp[MOFFT_MAX_STAGES];
   int count = chain_count;
@@ -734,6 +846,10 @@ mofft_status mofft_core_enqueue(const mofft_core *c, const void *in, void *out,
     a.split_shift = ps->split_shift;
     a.conj_in = backward && p == 0;
     a.conj_out = backward && p == P - 1;
+    if (ps->kind == MOFFT_KERNEL_TENSOR) {
+      a.aux = (const unsigned char *)c->d_twiddles + ps->aux_offset;
+      a.status = (int *)((unsigned char *)c->d_twiddles + ps->status_offset);
+    }
     a.generic_cols = P > 1;
     a.length = ps->length;
     a.lines = ps->lines;
@@ -793,6 +909,8 @@ mofft_status mofft_core_execute(const mofft_core *cc, const void *in, void *out)
       cudaGetLastError();
       st = MOFFT_INTERNAL_ERROR;
     }
+    if (st == MOFFT_SUCCESS && !c->user_stream && c->form != 0)
+      st = mofft_core_check_status(c);
   } else if (dev_in != dev_out) {
     st = MOFFT_INVALID_ARGUMENT; /* mixed host/device buffers */
   } else {
@@ -816,6 +934,7 @@ mofft_status mofft_core_execute(const mofft_core *cc, const void *in, void *out)
           st == MOFFT_SUCCESS)
         st = MOFFT_INTERNAL_ERROR;
       if (st != MOFFT_SUCCESS) cudaGetLastError();
+      if (st == MOFFT_SUCCESS && c->form != 0) st = mofft_core_check_status(c);
     }
     pthread_mutex_unlock(&c->lock);
   }
@@ -868,6 +987,50 @@ mofft_status mofft_schedule_preview(int precision_bits, size_t length,
     /* reference order: outermost radix first */
     for (int i = 0; i < count; ++i) chain_out[i] = chain[count - 1 - i];
     *chain_count = (size_t)count;
+  }
+  return MOFFT_SUCCESS;
+}
+
+/* Indirect batch: `batch` transforms, transform b read from in_table[b] and
+ * written to out_table[b] (device arrays of device pointers).  Out-of-place
+ * routing only (the second pass of a two-pass schedule runs in place on the
+ * output); schedules with a generic pass or more than two passes are not
+ * supported (MOFFT_UNSUPPORTED_SIZE). */
+mofft_status mofft_core_enqueue_indirect(const mofft_core *c, const void *const *in_table,
+                                         void *const *out_table, long long batch,
+                                         void *stream) {
+  const int P = c->sched.pass_count;
+  if (P > 2 || batch <= 0) return MOFFT_UNSUPPORTED_SIZE;
+  for (int p = 0; p < P; ++p)
+    if (c->sched.pass[p].kind == MOFFT_KERNEL_GENERIC ||
+        c->sched.pass[p].kind == MOFFT_KERNEL_TENSOR)
+      return MOFFT_UNSUPPORTED_SIZE;
+  const int backward = c->direction == MOFFT_BACKWARD;
+  for (int p = 0; p < P; ++p) {
+    const mofft_pass *ps = &c->sched.pass[p];
+    mofft_pass_args a;
+    memset(&a, 0, sizeof(a));
+    a.in_table = p == 0 ? in_table : (const void *const *)out_table;
+    a.out_table = out_table;
+    a.tw = (const unsigned char *)c->d_twiddles + ps->tw_offset;
+    a.tw_hi = (const unsigned char *)c->d_twiddles + ps->tw_hi_offset;
+    a.tw_lo = (const unsigned char *)c->d_twiddles + ps->tw_lo_offset;
+    a.batch = batch;
+    a.total = (long long)c->length;
+    a.ns_outer = ps->ns_outer;
+    a.split_shift = ps->split_shift;
+    a.conj_in = backward && p == 0;
+    a.conj_out = backward && p == P - 1;
+    a.length = ps->length;
+    a.lines = ps->lines;
+    a.radix_count = ps->radix_count;
+    memcpy(a.radices, ps->radices, sizeof(a.radices));
+    const int err = mofft_cuda_launch_pass(ps->kernel, &a, stream);
+    atomic_fetch_add(&g_launches, 1);
+    if (err != 0) {
+      cudaGetLastError();
+      return MOFFT_INTERNAL_ERROR;
+    }
   }
   return MOFFT_SUCCESS;
 }

@@ -18,7 +18,9 @@ extern "C" {
 typedef enum {
   MOFFT_KERNEL_ROWS = 0,    /* single pass, whole transforms per CTA */
   MOFFT_KERNEL_COLS = 1,    /* one pass of a multi-pass transform */
-  MOFFT_KERNEL_GENERIC = 2  /* runtime stage list, ROWS or COLS addressing */
+  MOFFT_KERNEL_GENERIC = 2, /* runtime stage list, ROWS or COLS addressing */
+  MOFFT_KERNEL_TENSOR = 3   /* whole transforms per CTA, DFT-matrix stages on
+                               the tensor cores (a precision form) */
 } mofft_kernel_kind;
 
 typedef struct {
@@ -32,6 +34,7 @@ typedef struct {
   int radix_count;      /* in-CTA Stockham stages, first to last */
   int radices[8];
   size_t smem_bytes;    /* dynamic shared memory per CTA */
+  int form;             /* mofft_precision_form; 0 for the CUDA-core kernels */
 } mofft_kernel_desc;
 
 typedef struct {
@@ -48,6 +51,15 @@ typedef struct {
   int split_shift;       /* COLS: log2 of the two-level twiddle split */
   int conj_in;           /* 1: negate imaginary part on load */
   int conj_out;          /* 1: negate imaginary part on store */
+  /* Indirect batch (device arrays of `batch` pointers, or NULL): transform b
+   * of this pass reads in_table[b] and writes out_table[b] (specialised
+   * kernels only). */
+  const void *const *in_table;
+  void *const *out_table;
+  /* tensor-core kernels only: constant B operand tiles and the error word
+   * the kernel sets when a wait on the tensor core timed out */
+  const void *aux;
+  int *status;
   /* generic kernel only */
   int generic_cols;      /* 0 ROWS addressing, 1 COLS addressing */
   int length;            /* line length L */
@@ -64,6 +76,12 @@ size_t mofft_cuda_generic_smem(int precision_bits, int length, int lines,
 /* Opt every kernel into its shared-memory size on the current device.
  * Returns a cudaError_t value (0 = success). */
 int mofft_cuda_prepare_device(void);
+/* Bytes of the B operand tiles of a tensor-core precision form (0 if the
+ * form has no tensor-core kernel), and their host-side construction from the
+ * 16-point forward DFT matrix fr + i fi (row-major F[k][r]). */
+size_t mofft_cuda_tensor_aux_bytes(int form);
+int mofft_cuda_tensor_fill_aux(int form, void *dst, const double *fr,
+                               const double *fi);
 /* Launch one pass on `stream` (a cudaStream_t).  Returns a cudaError_t. */
 int mofft_cuda_launch_pass(int kernel, const mofft_pass_args *args,
                            void *stream);

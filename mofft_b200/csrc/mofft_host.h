@@ -19,6 +19,11 @@ void mofft_cis_turns(uint64_t num, uint64_t den, long double *c,
 
 int mofft_group_chain(int precision_bits, unsigned bank, const int *chain,
                       int count, long long total, mofft_schedule *best);
+/* As mofft_group_chain, preferring the listed kernel instances (registry
+ * indices, MOFFT_MAX_PASSES entries, -1 = none) where they fit a pass. */
+int mofft_group_chain_preferred(int precision_bits, unsigned bank,
+                                const int *chain, int count, long long total,
+                                const int *preferred, mofft_schedule *best);
 int mofft_auto_radices(long long length, int *out, int capacity);
 int mofft_model_chain(int precision_bits, unsigned bank, size_t length,
                       int *chain, int capacity);
@@ -28,11 +33,22 @@ mofft_status mofft_core_create(mofft_core **out, int precision_bits,
                                mofft_direction direction,
                                mofft_placement placement, const int *chain,
                                int chain_count);
+mofft_status mofft_core_create_tuned(mofft_core **out, int precision_bits,
+                                     size_t length, size_t batch,
+                                     size_t distance, mofft_direction direction,
+                                     mofft_placement placement, const int *chain,
+                                     int chain_count, const int *preferred);
 mofft_status mofft_core_build(mofft_core *c);
+/* Blocking: MOFFT_INTERNAL_ERROR if a tensor-core kernel of c recorded a
+ * timed-out wait, else MOFFT_SUCCESS. */
+mofft_status mofft_core_check_status(const mofft_core *c);
 void mofft_core_destroy(mofft_core *c);
 mofft_status mofft_core_enqueue(const mofft_core *c, const void *in, void *out,
                                 void *stream);
 mofft_status mofft_core_execute(const mofft_core *c, const void *in, void *out);
+mofft_status mofft_core_enqueue_indirect(const mofft_core *c, const void *const *in_table,
+                                         void *const *out_table, long long batch,
+                                         void *stream);
 
 /* Twiddle tables (mofft_api.c): W_den^(first + k*step), k < count; the
  * internal stage table of an in-CTA chain; ceil(log2 x). */
@@ -53,9 +69,11 @@ mofft_status mofft_search_best(mofft_core **out, int precision_bits,
                                const mofft_plan_options *options,
                                mofft_plan_diagnostics *diagnostics);
 
-/* Compiled wisdom (device plan cache) lookup: returns chain length or 0. */
+/* Compiled wisdom (device plan cache) lookup: returns chain length or 0;
+ * `preferred` (MOFFT_MAX_PASSES entries, may be NULL) receives the tuned
+ * kernel instances as registry indices (-1 = none). */
 int mofft_wisdom_lookup(size_t length, int precision_bits, int *chain,
-                        int capacity);
+                        int capacity, int *preferred);
 
 #define MOFFT_KERNEL_BANK_COUNT 2u
 

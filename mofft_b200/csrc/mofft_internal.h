@@ -27,6 +27,8 @@ typedef struct {
   size_t tw_hi_offset;
   size_t tw_lo_offset;
   size_t smem_bytes;
+  size_t aux_offset;        /* tensor-core passes: B operand tiles */
+  size_t status_offset;     /* tensor-core passes: error word */
 } mofft_pass;
 
 typedef struct {
@@ -46,9 +48,16 @@ typedef struct mofft_core {
   int direct_input;
   mofft_stage_layout stage_layout;
   unsigned int kernel_bank;
+  /* Tuned kernel instances (registry indices, -1 = none) that the pass
+   * grouping prefers over the first matching instance: the autotuner's and
+   * the compiled wisdom's choice among variants of the same radix chain. */
+  int preferred[MOFFT_MAX_PASSES];
   const void *bound_input;
   void *bound_output;
   int has_bound_arrays;
+  /* precision form (mofft_precision_form); tensor-core forms replace the
+   * schedule with one tensor-core kernel and keep factors[] as they were */
+  int form;
   /* batched extension */
   size_t batch;
   size_t distance;

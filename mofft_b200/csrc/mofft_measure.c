@@ -26,6 +26,7 @@ typedef struct {
   int chain[MOFFT_MAX_STAGES];
   int count;
   unsigned bank;
+  int preferred[MOFFT_MAX_PASSES];   /* kernel instances to use, -1 = default */
   double model;
   double samples[32];
   double median;
@@ -49,14 +50,20 @@ static int same_candidate(const candidate *a, const candidate *b) {
   if (a->count != b->count || a->bank != b->bank) return 0;
   for (int i = 0; i < a->count; ++i)
     if (a->chain[i] != b->chain[i]) return 0;
+  for (int i = 0; i < MOFFT_MAX_PASSES; ++i)
+    if (a->preferred[i] != b->preferred[i]) return 0;
   return 1;
+}
+
+static void no_preference(candidate *c) {
+  for (int i = 0; i < MOFFT_MAX_PASSES; ++i) c->preferred[i] = -1;
 }
 
 /* Model score of a schedule: passes first, then generic kernels. */
 static double model_score(int precision_bits, const candidate *c, size_t length) {
   mofft_schedule s;
-  if (!mofft_group_chain(precision_bits, c->bank, c->chain, c->count,
-                         (long long)length, &s))
+  if (!mofft_group_chain_preferred(precision_bits, c->bank, c->chain, c->count,
+                                   (long long)length, c->preferred, &s))
     return INFINITY;
   double score = 0.0;
   for (int p = 0; p < s.pass_count; ++p)
@@ -79,6 +86,8 @@ static int model_compare(const void *l, const void *r) {
   if (a->count != b->count) return a->count < b->count ? -1 : 1;
   for (int i = 0; i < a->count; ++i)
     if (a->chain[i] != b->chain[i]) return a->chain[i] < b->chain[i] ? -1 : 1;
+  for (int i = 0; i < MOFFT_MAX_PASSES; ++i)
+    if (a->preferred[i] != b->preferred[i]) return a->preferred[i] < b->preferred[i] ? -1 : 1;
   return 0;
 }
 
@@ -96,6 +105,7 @@ static int enumerate(int precision_bits, size_t length, candidate *pool,
   candidate c;
   for (unsigned bank = 0; bank < MOFFT_KERNEL_BANK_COUNT; ++bank) {
     memset(&c, 0, sizeof(c));
+    no_preference(&c);
     c.bank = bank;
     c.count = mofft_model_chain(precision_bits, bank, length, c.chain,
                                 MOFFT_MAX_STAGES);
@@ -109,6 +119,8 @@ static int enumerate(int precision_bits, size_t length, candidate *pool,
         (size_t)d->length != length)
       continue;
     memset(&c, 0, sizeof(c));
+    no_preference(&c);
+    c.preferred[0] = i;
     c.bank = 0;
     c.count = d->radix_count;
     memcpy(c.chain, d->radices, (size_t)d->radix_count * sizeof(int));
@@ -127,19 +139,24 @@ static int enumerate(int precision_bits, size_t length, candidate *pool,
           (size_t)b->length != rest)
         continue;
       memset(&c, 0, sizeof(c));
+      no_preference(&c);
+      c.preferred[0] = i;
+      c.preferred[1] = j;
       c.bank = 0;
       memcpy(c.chain, a->radices, (size_t)a->radix_count * sizeof(int));
       memcpy(c.chain + a->radix_count, b->radices,
              (size_t)b->radix_count * sizeof(int));
       c.count = a->radix_count + b->radix_count;
       mofft_schedule s;
-      if (mofft_group_chain(precision_bits, 0, c.chain, c.count,
-                            (long long)length, &s))
+      if (mofft_group_chain_preferred(precision_bits, 0, c.chain, c.count,
+                                      (long long)length, c.preferred, &s) &&
+          s.pass_count == 2 && s.pass[0].kernel == i && s.pass[1].kernel == j)
         add_candidate(pool, &count, capacity, &c);
     }
   }
   /* the generic family with its default chain */
   memset(&c, 0, sizeof(c));
+  no_preference(&c);
   c.bank = 1;
   c.count = mofft_auto_radices((long long)length, c.chain, MOFFT_MAX_STAGES);
   if (c.count > 0) add_candidate(pool, &count, capacity, &c);
@@ -250,7 +267,10 @@ mofft_status mofft_search_best(mofft_core **out, int precision_bits,
         ((double *)h_in)[2 * i + 1] = im;
       }
     }
-    if (cudaMemcpy(d_in, h_in, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+    /* complete the upload before candidates launch on their own streams */
+    if (cudaMemcpy(d_in, h_in, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaDeviceSynchronize() != cudaSuccess) {
+      cudaGetLastError();
       status = MOFFT_INTERNAL_ERROR;
       goto done;
     }
@@ -260,8 +280,9 @@ mofft_status mofft_search_best(mofft_core **out, int precision_bits,
   for (size_t i = 0; i < nsel; ++i) {
     candidate *cand = &sel[i];
     mofft_core *c = NULL;
-    status = mofft_core_create(&c, precision_bits, length, batch, distance,
-                               direction, placement, cand->chain, cand->count);
+    status = mofft_core_create_tuned(&c, precision_bits, length, batch, distance,
+                                     direction, placement, cand->chain, cand->count,
+                                     cand->preferred);
     if (status == MOFFT_SUCCESS && cand->bank != 0) {
       c->kernel_bank = cand->bank;
       status = mofft_core_build(c);
@@ -308,8 +329,9 @@ mofft_status mofft_search_best(mofft_core **out, int precision_bits,
     }
   }
   qsort(sel, nsel, sizeof(candidate), time_compare);
-  status = mofft_core_create(out, precision_bits, length, batch, distance,
-                             direction, placement, sel[0].chain, sel[0].count);
+  status = mofft_core_create_tuned(out, precision_bits, length, batch, distance,
+                                   direction, placement, sel[0].chain, sel[0].count,
+                                   sel[0].preferred);
   if (status == MOFFT_SUCCESS && sel[0].bank != 0) {
     (*out)->kernel_bank = sel[0].bank;
     status = mofft_core_build(*out);

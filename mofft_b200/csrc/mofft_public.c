@@ -105,13 +105,14 @@ static mofft_status create_with_options(mofft_core **out, int precision_bits,
     return MOFFT_SUCCESS;
   }
   int chain[MOFFT_MAX_STAGES];
+  int preferred[MOFFT_MAX_PASSES];
   const int wisdom = mofft_wisdom_lookup(length, precision_bits, chain,
-                                         MOFFT_MAX_STAGES);
+                                         MOFFT_MAX_STAGES, preferred);
   if (!wisdom && (options.flags & MOFFT_PLAN_STRICT_WISDOM))
     return MOFFT_WISDOM_NOT_FOUND;
-  status = mofft_core_create(out, precision_bits, length, batch, distance,
-                             direction, placement, wisdom ? chain : NULL,
-                             wisdom);
+  status = mofft_core_create_tuned(out, precision_bits, length, batch, distance,
+                                   direction, placement, wisdom ? chain : NULL,
+                                   wisdom, preferred);
   if (status == MOFFT_SUCCESS && diagnostics) {
     diagnostics->used_wisdom = wisdom != 0;
     diagnostics->used_model_fallback = wisdom == 0;
@@ -202,6 +203,53 @@ static mofft_status set_kernel_bank(mofft_core *c, unsigned bank) {
     c->kernel_bank = old;
     if (mofft_core_build(c) != MOFFT_SUCCESS) st = MOFFT_INTERNAL_ERROR;
   }
+  if (saved >= 0 && saved != c->device) cudaSetDevice(saved);
+  return st;
+}
+
+/* Precision forms (FP32 plans only): tensor-core forms swap the schedule for
+ * one tensor-core kernel; on failure the previous form is rebuilt. */
+mofft_status mofft_plan_set_precision_form_f32(mofft_plan_f32 *plan,
+                                               mofft_precision_form form) {
+  if (!plan || (form != MOFFT_FORM_FP32 && form != MOFFT_FORM_TF32X3 &&
+                form != MOFFT_FORM_BF16X3))
+    return MOFFT_INVALID_ARGUMENT;
+  mofft_core *c = &plan->core;
+  if ((int)form == c->form) return MOFFT_SUCCESS;
+  const int old = c->form;
+  c->form = (int)form;
+  int saved = -1;
+  cudaGetDevice(&saved);
+  if (saved != c->device) cudaSetDevice(c->device);
+  mofft_status st = mofft_core_build(c);
+  if (st != MOFFT_SUCCESS) {
+    c->form = old;
+    if (mofft_core_build(c) != MOFFT_SUCCESS) st = MOFFT_INTERNAL_ERROR;
+  }
+  if (saved >= 0 && saved != c->device) cudaSetDevice(saved);
+  return st;
+}
+
+mofft_status mofft_plan_get_precision_form_f32(const mofft_plan_f32 *plan,
+                                               mofft_precision_form *form) {
+  if (!plan || !form) return MOFFT_INVALID_ARGUMENT;
+  *form = (mofft_precision_form)plan->core.form;
+  return MOFFT_SUCCESS;
+}
+
+mofft_status mofft_plan_check_f32(mofft_plan_f32 *plan) {
+  if (!plan) return MOFFT_INVALID_ARGUMENT;
+  mofft_core *c = &plan->core;
+  int saved = -1;
+  cudaGetDevice(&saved);
+  if (saved != c->device) cudaSetDevice(c->device);
+  void *stream = c->user_stream ? c->user_stream : c->stream;
+  mofft_status st = MOFFT_SUCCESS;
+  if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) {
+    cudaGetLastError();
+    st = MOFFT_INTERNAL_ERROR;
+  }
+  if (st == MOFFT_SUCCESS) st = mofft_core_check_status(c);
   if (saved >= 0 && saved != c->device) cudaSetDevice(saved);
   return st;
 }
@@ -412,9 +460,12 @@ static int options_from_bound_flags(uint32_t flags, mofft_plan_options *o) {
     if (!out || !valid_shape(direction, placement)) return MOFFT_INVALID_ARGUMENT; \
     *out = NULL;                                                                 \
     int chain[MOFFT_MAX_STAGES];                                                 \
-    const int wisdom = mofft_wisdom_lookup(length, BITS, chain, MOFFT_MAX_STAGES); \
-    return mofft_core_create((mofft_core **)out, BITS, length, 1, 0, direction, \
-                             placement, wisdom ? chain : NULL, wisdom);          \
+    int preferred[MOFFT_MAX_PASSES];                                             \
+    const int wisdom = mofft_wisdom_lookup(length, BITS, chain, MOFFT_MAX_STAGES, \
+                                           preferred);                           \
+    return mofft_core_create_tuned((mofft_core **)out, BITS, length, 1, 0,       \
+                                   direction, placement, wisdom ? chain : NULL,  \
+                                   wisdom, preferred);                           \
   }                                                                              \
   mofft_status mofft_plan_create_with_options_##SUF(                             \
       PLAN **out, size_t length, mofft_direction direction,                      \

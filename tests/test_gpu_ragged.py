@@ -1,0 +1,104 @@
+"""Ragged batches in one persistent launch (work-descriptor queue, CUDA
+graph): every item against the oracle, bit-identical repeats, each item the
+same alone and in the mix, and the per-item comparison path."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import mofft_b200 as m
+import oracle
+from mofft_b200 import workloads
+from tests.conftest import cuda_available, fp32_tol, rel_l2
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
+
+
+def make_items(spec, seed=0, inplace=lambda k: False):
+    """(source, output, direction, pristine input) per item; in-place items
+    have source is output."""
+    import torch
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    items = []
+    for k, (n, batch, direction) in enumerate(spec):
+        x = torch.view_as_complex(torch.rand((batch, n, 2), generator=gen, device="cuda") * 2 - 1)
+        if inplace(k):
+            y = x.clone()
+            items.append((y, y, direction, x))
+        else:
+            items.append((x, torch.empty_like(x), direction, x.clone()))
+    return items
+
+
+def test_ragged_matches_oracle_and_repeats():
+    import torch
+    # every length of the workload at least once, small batches
+    spec = [(n, 1 + (k % 5), -1 if k % 2 else 1) for k, n in enumerate(workloads.RAGGED_LENGTHS)]
+    spec += workloads.ragged_spec(count=24, seed=5, max_batch=6)
+    items = make_items(spec, inplace=lambda k: k % 3 == 1)
+    plan = m.RaggedPlan([(a, b, d) for a, b, d, _ in items])
+    tiles, grid = plan.info()
+    assert tiles > 0 and grid > 0
+    plan.execute()
+    torch.cuda.synchronize()
+    assert plan.status() == 0
+    first = [b.clone() for _, b, _, _ in items]
+    for (src, out, direction, orig), got in zip(items, first):
+        x = orig.cpu().numpy()
+        ref = oracle.fft_ld(x.astype(np.complex128), direction)
+        n = x.shape[-1]
+        assert rel_l2(got.cpu().numpy(), ref) <= fp32_tol(n), (n, direction)
+    # repeat (graph replay): restore in-place inputs, results bit-identical
+    for src, out, direction, orig in items:
+        if src.data_ptr() == out.data_ptr():
+            out.copy_(orig)
+    plan.execute()
+    torch.cuda.synchronize()
+    assert plan.status() == 0
+    for (_, out, _, _), got in zip(items, first):
+        assert torch.equal(out, got)
+    plan.destroy()
+
+
+def test_item_alone_equals_item_in_mix():
+    import torch
+    spec = workloads.ragged_spec(count=40, seed=9, max_batch=4)
+    items = make_items(spec, seed=1)
+    mix = m.RaggedPlan([(a, b, d) for a, b, d, _ in items])
+    mix.execute()
+    torch.cuda.synchronize()
+    assert mix.status() == 0
+    for k in (0, 7, 19, 39):
+        _, y_mix, direction, x = items[k]
+        y_alone = torch.empty_like(x)
+        alone = m.RaggedPlan([(x, y_alone, direction)])
+        alone.execute()
+        torch.cuda.synchronize()
+        assert alone.status() == 0
+        assert torch.equal(y_alone, y_mix), spec[k]
+        alone.destroy()
+    mix.destroy()
+
+
+def test_per_item_path_agrees():
+    import torch
+    spec = workloads.ragged_spec(count=32, seed=3, max_batch=4)
+    items = make_items(spec, seed=2)
+    plan = m.RaggedPlan([(a, b, d) for a, b, d, _ in items])
+    plan.execute()
+    torch.cuda.synchronize()
+    ragged = [b.clone() for _, b, _, _ in items]
+    plan.execute_per_item()
+    torch.cuda.synchronize()
+    for (_, out, _, _), r in zip(items, ragged):
+        n = out.shape[-1]
+        assert rel_l2(out.cpu().numpy(), r.cpu().numpy()) <= fp32_tol(n)
+    plan.destroy()
+
+
+def test_unsupported_length_rejected():
+    import torch
+    x = torch.zeros((1, 17 * 16), dtype=torch.complex64, device="cuda")
+    with pytest.raises(m.MofftError):
+        m.RaggedPlan([(x, x, -1)])

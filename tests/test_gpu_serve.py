@@ -1,0 +1,105 @@
+"""Serving loop (include/mofft_serve.h): results of a request mix against
+the oracle, each result bit-identical alone and in the mix, coalescing into
+fewer launches than requests, host and device buffers, admission cap."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import mofft_b200 as m
+import oracle
+from tests.conftest import cuda_available, fp32_tol, fp64_tol, rel_l2
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
+
+
+def _tensor(batch, n, bits, seed):
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    dt = torch.float32 if bits == 32 else torch.float64
+    return torch.view_as_complex(torch.rand((batch, n, 2), generator=g, device="cuda",
+                                            dtype=dt) * 2 - 1)
+
+
+def test_mix_matches_oracle_host_and_device():
+    import torch
+    srv = m.Server(streams=4)
+    reqs = []
+    rng = np.random.default_rng(0)
+    for k in range(48):
+        n = int(2 ** rng.integers(8, 21))
+        bits = 32 if k % 5 else 64
+        batch = int(rng.integers(1, 4))
+        d = -1 if k % 2 else 1
+        x = _tensor(batch, n, bits, k)
+        if k % 3 == 0:      # host (pinned) buffers
+            hx = x.cpu().pin_memory()
+            hy = torch.empty_like(hx).pin_memory()
+            t = srv.submit(n, batch, d, bits, hx.data_ptr(), hy.data_ptr())
+            reqs.append((t, x, hy, d, n, bits, hx))     # inputs must outlive the request
+        elif k % 3 == 1:    # device, in place
+            y = x.clone()
+            t = srv.submit(n, batch, d, bits, y.data_ptr(), y.data_ptr())
+            reqs.append((t, x, y, d, n, bits, None))
+        else:               # device, out of place
+            y = torch.empty_like(x)
+            t = srv.submit(n, batch, d, bits, x.data_ptr(), y.data_ptr())
+            reqs.append((t, x, y, d, n, bits, None))
+    for t, x, y, d, n, bits, _ in reqs:
+        st, lat = srv.wait(t)
+        assert st == 0 and lat > 0
+        torch.cuda.synchronize()
+        got = y.cpu().numpy()[:1]
+        ref = oracle.fft_ld(x.cpu().numpy()[:1].astype(np.complex128), d)
+        assert rel_l2(got, ref) <= (fp32_tol(n) if bits == 32 else fp64_tol(n)), (n, bits, d)
+    stats = srv.stats()
+    assert stats["completed"] == 48 and stats["failed"] == 0
+    srv.destroy()
+
+
+@pytest.mark.parametrize("n", [1024, 65536])
+def test_alone_equals_mix_and_coalesces(n):
+    import torch
+    x = _tensor(3, n, 32, 7)
+    alone_out = torch.empty_like(x)
+    srv = m.Server(streams=2)
+    st, _ = srv.wait(srv.submit(n, 3, -1, 32, x.data_ptr(), alone_out.data_ptr()))
+    assert st == 0
+    srv.destroy()
+    # the same request in a mix of 64 same-length requests submitted together
+    srv = m.Server(streams=1)
+    others = [(_tensor(2, n, 32, 100 + k), None) for k in range(64)]
+    outs = [torch.empty_like(o) for o, _ in others]
+    tickets = []
+    for k, ((o, _), out) in enumerate(zip(others, outs)):
+        if k == 20:
+            mix_out = torch.empty_like(x)
+            tickets.append(srv.submit(n, 3, -1, 32, x.data_ptr(), mix_out.data_ptr()))
+        tickets.append(srv.submit(n, 2, -1, 32, o.data_ptr(), out.data_ptr()))
+    for t in tickets:
+        assert srv.wait(t)[0] == 0
+    torch.cuda.synchronize()
+    assert torch.equal(alone_out, mix_out)
+    stats = srv.stats()
+    assert stats["launches"] < len(tickets)       # requests were coalesced
+    srv.destroy()
+
+
+def test_admission_cap():
+    import torch
+    n, batch = 4096, 64
+    x = _tensor(batch, n, 32, 3)
+    y = torch.empty_like(x)
+    payload = 2 * batch * n * 8
+    srv = m.Server(hbm_budget_bytes=payload)        # room for exactly one request
+    small = [srv.submit(n, batch, -1, 32, x.data_ptr(), y.data_ptr()) for _ in range(4)]
+    for t in small:
+        assert srv.wait(t)[0] == 0
+    big = _tensor(2 * batch, n, 32, 4)
+    t = srv.submit(n, 2 * batch, -1, 32, big.data_ptr(), big.data_ptr())
+    assert srv.wait(t)[0] == m.Status.ALLOCATION_FAILURE
+    assert srv.stats()["peak_admitted_bytes"] <= payload
+    with pytest.raises(m.MofftError):
+        srv.submit(17 * 16, 1, -1, 32, x.data_ptr(), y.data_ptr())
+    srv.destroy()

@@ -1,0 +1,151 @@
+"""Tensor-core precision forms of the n = 4096 FP32 transform.
+
+MOFFT_FORM_TF32X3 and MOFFT_FORM_BF16X3 run the three radix-16 Stockham
+stages as DFT-matrix GEMMs on the tcgen05 tensor cores with split operands
+(hi + lo, three products, FP32 accumulation).  They are checked against the
+long-double oracle on the precision-mix inputs (a third uniform[-1,1), a
+third log-uniform magnitudes 1e-3..1e3 with uniform phase, a third single
+tones), forward and backward, in place and out of place, through the C-ABI.
+
+Tolerances (relative L2 error over the batch, written here because the forms
+are not FP32-exact):
+  TF32X3  every operand carries 2 x 11 significant bits, so a product is
+          good to about 3 * 2^-22; three stages: rel-L2 <= 4e-6.
+  BF16X3  2 x 8 bits, about 3 * 2^-18 per product: rel-L2 <= 1e-4.
+The CUDA-core FP32 path of the same plan must stay within the FP32 bound
+(5e-7 * log2 n) and be at least as accurate as TF32X3, which must in turn be
+more accurate than BF16X3."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import mofft_b200 as m
+import oracle
+from mofft_b200 import workloads
+from tests.conftest import cuda_available, fp32_tol, rel_l2
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
+
+N = 4096
+TOL = {m.FORM_TF32X3: 4e-6, m.FORM_BF16X3: 1e-4}
+NAMES = {m.FORM_TF32X3: "tf32x3", m.FORM_BF16X3: "bf16x3"}
+
+
+def _mix(batch: int, seed: int = 3) -> np.ndarray:
+    return workloads.precision_mix(batch * N, N, seed=seed)
+
+
+def _expected(x: np.ndarray, direction: int) -> np.ndarray:
+    return oracle.fft_ld(x.astype(np.complex128), direction)
+
+
+def _run(x: np.ndarray, direction: int, placement: int, form: int) -> np.ndarray:
+    import torch
+    batch = x.shape[0]
+    d = torch.from_numpy(x).cuda()
+    out = d if placement == m.IN_PLACE else torch.empty_like(d)
+    with m.Plan.create(N, direction, placement, bits=32, batch=batch) as plan:
+        plan.set_precision_form(form)
+        assert plan.precision_form == form
+        plan.execute(d, out)
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize("form", [m.FORM_TF32X3, m.FORM_BF16X3])
+@pytest.mark.parametrize("direction", [m.FORWARD, m.BACKWARD])
+@pytest.mark.parametrize("placement", [m.OUT_OF_PLACE, m.IN_PLACE])
+def test_form_matches_oracle(form, direction, placement):
+    x = _mix(24)
+    want = _expected(x, direction)
+    got = _run(x, direction, placement, form)
+    err = rel_l2(got, want)
+    assert err <= TOL[form], (NAMES[form], direction, placement, err)
+    # every input class of the mix within the bound on its own
+    third = x.shape[0] // 3
+    for lo, hi in ((0, third), (third, 2 * third), (2 * third, x.shape[0])):
+        e = rel_l2(got[lo:hi], want[lo:hi])
+        assert e <= TOL[form], (NAMES[form], lo, e)
+
+
+def test_error_ordering_fp32_tf32x3_bf16x3():
+    x = _mix(12, seed=9)
+    want = _expected(x, m.FORWARD)
+    errs = {f: rel_l2(_run(x, m.FORWARD, m.OUT_OF_PLACE, f), want)
+            for f in (m.FORM_FP32, m.FORM_TF32X3, m.FORM_BF16X3)}
+    print("rel-L2 vs oracle:", {("fp32", "tf32x3", "bf16x3")[f]: f"{e:.3e}"
+                                for f, e in errs.items()})
+    assert errs[m.FORM_FP32] <= fp32_tol(N)
+    assert errs[m.FORM_FP32] <= errs[m.FORM_TF32X3] * 1.5
+    assert errs[m.FORM_TF32X3] < errs[m.FORM_BF16X3]
+
+
+def test_roundtrip_and_repeat_bitwise():
+    import torch
+    x = _mix(6, seed=4)
+    d = torch.from_numpy(x).cuda()
+    y1 = torch.empty_like(d)
+    y2 = torch.empty_like(d)
+    z = torch.empty_like(d)
+    with m.Plan.create(N, m.FORWARD, m.OUT_OF_PLACE, bits=32, batch=6) as fwd, \
+            m.Plan.create(N, m.BACKWARD, m.OUT_OF_PLACE, bits=32, batch=6) as bwd:
+        fwd.set_precision_form(m.FORM_TF32X3)
+        bwd.set_precision_form(m.FORM_TF32X3)
+        fwd.execute(d, y1)
+        fwd.execute(d, y2)
+        bwd.execute(y1, z)
+    assert torch.equal(y1, y2)            # deterministic
+    back = z.cpu().numpy() / N
+    assert rel_l2(back, x) <= 2 * TOL[m.FORM_TF32X3]
+
+
+def test_schedule_switch_and_unsupported_length():
+    kernels = {k["index"]: k for k in m.kernels()}
+    tensor = [k for k in kernels.values() if k["kind"] == m.KERNEL_TENSOR]
+    assert sorted(k["name"] for k in tensor) == ["tensor_float_4096_bf16x3_r16x3",
+                                                "tensor_float_4096_tf32x3_r16x3"]
+    with m.Plan.create(N, m.FORWARD, m.OUT_OF_PLACE, bits=32, batch=4) as plan:
+        base = plan.schedule()
+        plan.set_precision_form(m.FORM_BF16X3)
+        s = plan.schedule()
+        assert s["pass_count"] == 1
+        assert kernels[s["kernels"][0]]["name"] == "tensor_float_4096_bf16x3_r16x3"
+        plan.set_precision_form(m.FORM_FP32)
+        assert plan.schedule()["kernels"] == base["kernels"]
+    with m.Plan.create(2048, m.FORWARD, m.OUT_OF_PLACE, bits=32, batch=4) as plan:
+        with pytest.raises(m.MofftError) as e:
+            plan.set_precision_form(m.FORM_TF32X3)
+        assert e.value.status == m.Status.UNSUPPORTED_SIZE
+        assert plan.precision_form == m.FORM_FP32
+        plan.execute(*_pair(2048, 4))      # still runs its FP32 schedule
+
+
+def _pair(n, batch):
+    import torch
+    x = torch.ones((batch, n), dtype=torch.complex64, device="cuda")
+    return x, torch.empty_like(x)
+
+
+def test_host_buffers_distance_and_stream():
+    import torch
+    batch, dist = 5, N + 96
+    x = np.zeros((batch, dist), dtype=np.complex64)
+    x[:, :N] = _mix(batch, seed=8)[:batch]
+    want = _expected(x[:, :N], m.BACKWARD)
+    y = np.zeros_like(x)
+    with m.Plan.create(N, m.BACKWARD, m.OUT_OF_PLACE, bits=32, batch=batch,
+                       distance=dist) as plan:
+        plan.set_precision_form(m.FORM_TF32X3)
+        plan.execute(x, y)                  # host buffers: staged copies
+        assert rel_l2(y[:, :N], want) <= TOL[m.FORM_TF32X3]
+        d = torch.from_numpy(x).cuda()
+        o = torch.zeros_like(d)
+        stream = torch.cuda.Stream()
+        plan.set_stream(stream.cuda_stream)
+        with torch.cuda.stream(stream):
+            plan.execute(d, o)              # asynchronous on the attached stream
+        plan.check_status()                 # blocking; no wait timed out
+        got = o.cpu().numpy()
+    assert rel_l2(got[:, :N], want) <= TOL[m.FORM_TF32X3]
+    assert not np.any(got[:, N:])           # padding between transforms untouched

@@ -188,6 +188,18 @@ def test_kernel_registry_is_consistent():
                        k["precision_bits"] == bits for k in ks), (bits, n)
 
 
+def test_tensor_forms_registered_and_never_planned():
+    ks = m.kernels()
+    tensor = sorted((k["name"], k["length"], k["radices"], k["precision_bits"])
+                    for k in ks if k["kind"] == m.KERNEL_TENSOR)
+    assert tensor == [("tensor_float_4096_bf16x3_r16x3", 4096, [16, 16, 16], 32),
+                      ("tensor_float_4096_tf32x3_r16x3", 4096, [16, 16, 16], 32)]
+    # the planner keeps FP32 (CUDA-core) kernels unless a form is requested
+    for bits in (32, 64):
+        s = m.schedule_preview(4096, bits)
+        assert all(ks[k]["kind"] != m.KERNEL_TENSOR for k in s["kernels"])
+
+
 def test_mixed_lengths_use_specialised_kernels():
     """3*2^k and 5*2^k lengths of the plain-method sweep run on specialised
     kernels (no runtime-stage kernel), single pass up to 12288 / 10240."""
