@@ -338,7 +338,43 @@ __device__ __forceinline__ void rows_body(const RowsArgs<T>& a, long long b0,
   lay.gin = lay.active ? batch_in<T>(a.in, a.in_dist, a.in_table, b) : a.in;
   lay.gout = lay.active ? batch_out<T>(a.out, a.out_dist, a.out_table, b) : a.out;
   lay.sign = a.sign;
-  if (STAGED) {
+  // Dense full tile: the TB lines are one contiguous, 16-byte aligned block
+  // of TB*L elements, copied with unrolled 16-byte vector accesses so that a
+  // thread has all of its loads in flight at once.
+  constexpr int kThreadsTile = TPL * TB;
+  constexpr int kVecs = (int)(TB * L * sizeof(cplx_t<T>) / 16);
+  constexpr int kPer = kVecs / kThreadsTile;
+  constexpr int kPerVec = (int)(16 / sizeof(cplx_t<T>));      // elements per vector
+  constexpr bool kVecOk = STAGED && kVecs % kThreadsTile == 0 && kPer <= 16 &&
+                          (TB * L * sizeof(cplx_t<T>)) % 16 == 0;
+  bool dense = false;
+  if constexpr (kVecOk) {
+    dense = a.in_table == nullptr && a.out_table == nullptr && a.in_dist == L &&
+            a.out_dist == L && b0 + TB <= a.batch &&
+            ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.out)) & 15) == 0;
+  }
+  if constexpr (kVecOk) {
+    if (dense) {
+      const uint4* src = reinterpret_cast<const uint4*>(a.in + b0 * L);
+      uint4 v[kPer > 0 ? kPer : 1];
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) v[k] = __ldcg(src + threadIdx.x + k * kThreadsTile);
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) {
+        const cplx_t<T>* c = reinterpret_cast<const cplx_t<T>*>(&v[k]);
+#pragma unroll
+        for (int e = 0; e < kPerVec; ++e) {
+          const int q = (threadIdx.x + k * kThreadsTile) * kPerVec + e;
+          const int ln = q / L;
+          const int i = q - ln * L;
+          sre[ln * LINE + spad<T>(i)] = c[e].x;
+          sim[ln * LINE + spad<T>(i)] = c[e].y * a.sign;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (STAGED && !dense) {
     // Cooperative load of lines b0 .. b0+TB-1 (each L contiguous elements).
     const long long lines = (a.batch - b0) < TB ? (a.batch - b0) : TB;
     for (int q = threadIdx.x; q < TB * L; q += TPL * TB) {
@@ -354,7 +390,26 @@ __device__ __forceinline__ void rows_body(const RowsArgs<T>& a, long long b0,
     __syncthreads();
   }
   StageRunner<T, L, TPL, 1, 0, STAGED, STAGED, true, DTW, Rs...>::run(lay, t, a.tw);
-  if (STAGED) {
+  if constexpr (kVecOk) {
+    if (dense) {
+      uint4* dst = reinterpret_cast<uint4*>(a.out + b0 * L);
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) {
+        uint4 v;
+        cplx_t<T>* c = reinterpret_cast<cplx_t<T>*>(&v);
+#pragma unroll
+        for (int e = 0; e < kPerVec; ++e) {
+          const int q = (threadIdx.x + k * kThreadsTile) * kPerVec + e;
+          const int ln = q / L;
+          const int i = q - ln * L;
+          c[e].x = sre[ln * LINE + spad<T>(i)];
+          c[e].y = sim[ln * LINE + spad<T>(i)] * a.sign;
+        }
+        dst[threadIdx.x + k * kThreadsTile] = v;
+      }
+    }
+  }
+  if (STAGED && !dense) {
     const long long lines = (a.batch - b0) < TB ? (a.batch - b0) : TB;
     for (int q = threadIdx.x; q < TB * L; q += TPL * TB) {
       const int ln = q / L;
