@@ -167,6 +167,7 @@ struct ColsLayout {
 // Kernel flags (template parameter FLAGS of the ROWS kernels).
 constexpr int kStaged = 1;       // I/O staged through shared memory
 constexpr int kDerivedTw = 2;    // radix-16 twiddles from w, w^2, w^4, w^8
+constexpr int kSplitX = 4;       // exchanges move one component at a time
 
 // Twiddles of one radix-16 butterfly: v[r] *= w^r.  Loads the table entries
 // of w^1, w^2, w^4 and w^8 and forms the other powers with at most three
@@ -284,6 +285,112 @@ struct StageRunner<T, L, TPL, NS, TWOFF, FS, LS, IS_FIRST, DTW, R, R2, Rest...> 
 };
 
 // ---------------------------------------------------------------------------
+// Split-exchange stage chain (FLAGS & kSplitX, one-pass kernels with direct
+// global I/O).  Values stay in registers between stages and each exchange
+// moves the real parts through a single shared buffer, then the imaginary
+// parts through the same buffer, so a line needs L words of shared memory
+// instead of 2L: twice the resident CTAs for the long one-pass lengths.
+// ---------------------------------------------------------------------------
+template <typename T, int R, int NS, int TWOFF, bool DTW, int PER, int TPL>
+__device__ __forceinline__ void split_compute(T (&vr)[PER][R], T (&vi)[PER][R], int t,
+                                              const cplx_t<T>* __restrict__ tw) {
+#pragma unroll
+  for (int m = 0; m < PER; ++m) {
+    const int j = t + m * TPL;
+    if (NS > 1) {
+      const int jm = j % NS;
+      if constexpr (DTW && R == 16) {
+        twiddle16_derived<T, NS, TWOFF>(vr[m], vi[m], jm, tw);
+      } else {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          const cplx_t<T> w = __ldg(tw + TWOFF + (r - 1) * NS + jm);
+          cmul<T>(vr[m][r], vi[m][r], w.x, w.y);
+        }
+      }
+    }
+    Dft<R>::fwd(vr[m], vi[m]);
+  }
+}
+
+// Stockham output positions of stage (R, NS): y[(j/NS) NS R + j%NS + k NS].
+template <typename T, int R, int NS, int PER, int TPL>
+__device__ __forceinline__ void split_put(T* buf, const T (&v)[PER][R], int t) {
+#pragma unroll
+  for (int m = 0; m < PER; ++m) {
+    const int j = t + m * TPL;
+    const int base = (j / NS) * NS * R + (j % NS);
+#pragma unroll
+    for (int k = 0; k < R; ++k) buf[spad<T>(base + k * NS)] = v[m][k];
+  }
+}
+
+// Input positions of stage (R, *) of an L-point line: x[j + r L/R].
+template <typename T, int L, int R, int PER, int TPL>
+__device__ __forceinline__ void split_get(const T* buf, T (&v)[PER][R], int t) {
+  constexpr int BF = L / R;
+#pragma unroll
+  for (int m = 0; m < PER; ++m) {
+    const int j = t + m * TPL;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[m][r] = buf[spad<T>(j + r * BF)];
+  }
+}
+
+template <typename T, int L, int TPL, int NS, int TWOFF, bool DTW, int R, int... Rest>
+struct SplitRunner {
+  static constexpr int PER = (L / R) / TPL;
+  static_assert((L / R) % TPL == 0, "split exchange needs whole butterflies per thread");
+  __device__ __forceinline__ static void run(T* buf, const RowsLayout<T>& lay, int t,
+                                             const cplx_t<T>* tw, T (&vr)[PER][R],
+                                             T (&vi)[PER][R]) {
+    split_compute<T, R, NS, TWOFF, DTW, PER, TPL>(vr, vi, t, tw);
+    if constexpr (sizeof...(Rest) == 0) {
+#pragma unroll
+      for (int m = 0; m < PER; ++m) {
+        const int j = t + m * TPL;
+        const int base = (j / NS) * NS * R + (j % NS);
+#pragma unroll
+        for (int k = 0; k < R; ++k) lay.gstore(base + k * NS, vr[m][k], vi[m][k]);
+      }
+    } else {
+      using Next = SplitRunner<T, L, TPL, NS * R, TWOFF + stage_table_size(R, NS), DTW, Rest...>;
+      constexpr int R2 = Next::kRadix;
+      T nr[Next::PER][R2];
+      T ni[Next::PER][R2];
+      split_put<T, R, NS, PER, TPL>(buf, vr, t);
+      __syncthreads();
+      split_get<T, L, R2, Next::PER, TPL>(buf, nr, t);
+      __syncthreads();
+      split_put<T, R, NS, PER, TPL>(buf, vi, t);
+      __syncthreads();
+      split_get<T, L, R2, Next::PER, TPL>(buf, ni, t);
+      __syncthreads();
+      Next::run(buf, lay, t, tw, nr, ni);
+    }
+  }
+  static constexpr int kRadix = R;
+};
+
+// One-pass tile with split exchanges: first stage loads global memory,
+// last stage stores it, shared memory holds one component per line.
+template <typename T, int L, int TPL, int TB, bool DTW, int R0, int... Rs>
+__device__ __forceinline__ void rows_body_split(const RowsLayout<T>& lay, T* buf, int t,
+                                                const cplx_t<T>* tw) {
+  using First = SplitRunner<T, L, TPL, 1, 0, DTW, R0, Rs...>;
+  constexpr int BF = L / R0;
+  T vr[First::PER][R0];
+  T vi[First::PER][R0];
+#pragma unroll
+  for (int m = 0; m < First::PER; ++m) {
+    const int j = t + m * TPL;
+#pragma unroll
+    for (int r = 0; r < R0; ++r) lay.gload(j + r * BF, vr[m][r], vi[m][r]);
+  }
+  First::run(buf, lay, t, tw, vr, vi);
+}
+
+// ---------------------------------------------------------------------------
 // ROWS kernel: single pass.  A CTA computes TB complete transforms of length
 // L (each by TPL threads).  With STAGED, the CTA's TB*L contiguous input
 // elements are first copied to shared memory with coalesced vector loads and
@@ -389,7 +496,12 @@ __device__ __forceinline__ void rows_body(const RowsArgs<T>& a, long long b0,
     }
     __syncthreads();
   }
-  StageRunner<T, L, TPL, 1, 0, STAGED, STAGED, true, DTW, Rs...>::run(lay, t, a.tw);
+  if constexpr ((FLAGS & kSplitX) != 0) {
+    static_assert(!STAGED, "split exchanges run with direct global I/O");
+    rows_body_split<T, L, TPL, TB, DTW, Rs...>(lay, sre + line * LINE, t, a.tw);
+  } else {
+    StageRunner<T, L, TPL, 1, 0, STAGED, STAGED, true, DTW, Rs...>::run(lay, t, a.tw);
+  }
   if constexpr (kVecOk) {
     if (dense) {
       uint4* dst = reinterpret_cast<uint4*>(a.out + b0 * L);

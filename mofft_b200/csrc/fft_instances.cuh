@@ -55,7 +55,7 @@ ColsArgs<T> cols_args(const mofft_pass_args *p) {
 template <typename T, int L, int TPL, int TB, int FLAGS, int... Rs>
 struct RowsInst {
   static constexpr size_t smem() {
-    return 2ull * TB * spad_len<T>(L) * sizeof(T);
+    return ((FLAGS & kSplitX) ? 1ull : 2ull) * TB * spad_len<T>(L) * sizeof(T);
   }
   static const void *func() {
     return reinterpret_cast<const void *>(&rows_kernel<T, L, TPL, TB, FLAGS, Rs...>);
@@ -209,6 +209,9 @@ struct GenericInst {
 #define ROWSD(T, L, TPL, TB, ST, ...) \
   RowsInst<T, L, TPL, TB, ((ST) ? kStaged : 0) | kDerivedTw, __VA_ARGS__>::entry( \
       "rows_" #T "_" #L "_t" #TPL "_b" #TB "_s" #ST "_d")
+#define ROWSX(T, L, TPL, TB, ...) \
+  RowsInst<T, L, TPL, TB, kDerivedTw | kSplitX, __VA_ARGS__>::entry( \
+      "rows_" #T "_" #L "_t" #TPL "_b" #TB "_sfalse_dx")
 #define COLS(T, L, TPL, C, ...) \
   ColsInst<T, L, TPL, C, __VA_ARGS__>::entry("cols_" #T "_" #L "_t" #TPL "_c" #C)
 

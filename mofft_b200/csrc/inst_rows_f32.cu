@@ -33,6 +33,12 @@ const Entry *entries_rows_f32(int *count) {
       ROWSD(float, 4096, 512, 1, false, 16, 16, 16),
       ROWSD(float, 8192, 512, 1, false, 16, 16, 16, 2),
       ROWSD(float, 16384, 512, 1, false, 16, 16, 16, 4),
+      // split exchanges (one component at a time: half the shared memory)
+      ROWSX(float, 2048, 128, 2, 16, 16, 8),
+      ROWSX(float, 4096, 256, 1, 16, 16, 16),
+      ROWSX(float, 8192, 512, 1, 16, 16, 16, 2),
+      ROWSX(float, 16384, 512, 1, 16, 16, 16, 4),
+      ROWSX(float, 16384, 1024, 1, 16, 16, 16, 4),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;

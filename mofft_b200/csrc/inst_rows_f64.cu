@@ -23,6 +23,9 @@ const Entry *entries_rows_f64(int *count) {
       ROWSD(double, 1024, 64, 2, false, 16, 16, 4),
       ROWSD(double, 4096, 256, 1, false, 16, 16, 16),
       ROWSD(double, 8192, 512, 1, false, 16, 16, 16, 2),
+      ROWSX(double, 2048, 128, 2, 16, 16, 8),
+      ROWSX(double, 4096, 256, 1, 16, 16, 16),
+      ROWSX(double, 8192, 512, 1, 16, 16, 16, 2),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;
