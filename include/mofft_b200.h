@@ -155,6 +155,15 @@ typedef enum {
   MOFFT_FORM_TF32X3 = 1,
   MOFFT_FORM_BF16X3 = 2
 } mofft_precision_form;
+/* The form can also be chosen at creation: these bits of
+ * mofft_plan_options.flags (PRETUNED mode, FP32 plans; at most one of them)
+ * create the plan with that form.  With an FP64 plan, with MEASURE or with
+ * both bits the options are MOFFT_INVALID_ARGUMENT; a length without a
+ * tensor-core kernel gives MOFFT_UNSUPPORTED_SIZE. */
+enum {
+  MOFFT_PLAN_FORM_TF32X3 = 1u << 8,
+  MOFFT_PLAN_FORM_BF16X3 = 1u << 9
+};
 mofft_status mofft_plan_set_precision_form_f32(mofft_plan_f32 *plan,
                                                mofft_precision_form form);
 mofft_status mofft_plan_get_precision_form_f32(const mofft_plan_f32 *plan,

@@ -44,6 +44,8 @@ PLANNER_MEASURE = 1
 FORM_FP32 = 0
 FORM_TF32X3 = 1
 FORM_BF16X3 = 2
+PLAN_FORM_TF32X3 = 1 << 8    # mofft_plan_options.flags bits
+PLAN_FORM_BF16X3 = 1 << 9
 PLAN_STRICT_WISDOM = 1
 FLAG_PRETUNED = 0
 FLAG_MEASURE = 1

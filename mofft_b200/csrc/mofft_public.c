@@ -36,15 +36,18 @@ void mofft_plan_options_init(mofft_plan_options *options) {
   options->timing_samples = 0;
 }
 
+#define FORM_BITS ((uint32_t)MOFFT_PLAN_FORM_TF32X3 | (uint32_t)MOFFT_PLAN_FORM_BF16X3)
+
 /* Same acceptance rules as the reference's validate_options
- * (src/mofft.c:739-762). */
+ * (src/mofft.c:739-762); the precision-form bits are this library's. */
 static mofft_status validate_options(const mofft_plan_options *given,
                                      mofft_plan_options *resolved) {
   if (given) *resolved = *given;
   else mofft_plan_options_init(resolved);
   if ((resolved->mode != MOFFT_PLANNER_PRETUNED &&
        resolved->mode != MOFFT_PLANNER_MEASURE) ||
-      (resolved->flags & ~((uint32_t)MOFFT_PLAN_STRICT_WISDOM)) != 0 ||
+      (resolved->flags & ~((uint32_t)MOFFT_PLAN_STRICT_WISDOM | FORM_BITS)) != 0 ||
+      (resolved->flags & FORM_BITS) == FORM_BITS ||
       (resolved->mode == MOFFT_PLANNER_MEASURE && resolved->flags != 0))
     return MOFFT_INVALID_ARGUMENT;
   if (resolved->candidate_limit == 0)
@@ -91,6 +94,10 @@ static mofft_status create_with_options(mofft_core **out, int precision_bits,
   mofft_plan_options options;
   mofft_status status = validate_options(given, &options);
   if (status != MOFFT_SUCCESS) return status;
+  const int form = (options.flags & MOFFT_PLAN_FORM_TF32X3)   ? MOFFT_FORM_TF32X3
+                   : (options.flags & MOFFT_PLAN_FORM_BF16X3) ? MOFFT_FORM_BF16X3
+                                                              : MOFFT_FORM_FP32;
+  if (form != MOFFT_FORM_FP32 && precision_bits != 32) return MOFFT_INVALID_ARGUMENT;
   if (!mofft_hardware_supports(precision_bits)) return MOFFT_UNSUPPORTED_HARDWARE;
   const double start = mofft_monotonic_seconds();
   if (start < 0.0) return MOFFT_INTERNAL_ERROR;
@@ -113,6 +120,15 @@ static mofft_status create_with_options(mofft_core **out, int precision_bits,
   status = mofft_core_create_tuned(out, precision_bits, length, batch, distance,
                                    direction, placement, wisdom ? chain : NULL,
                                    wisdom, preferred);
+  if (status == MOFFT_SUCCESS && form != MOFFT_FORM_FP32) {
+    (*out)->form = form;
+    status = mofft_core_build(*out);
+    if (status != MOFFT_SUCCESS) {
+      mofft_core_destroy(*out);
+      *out = NULL;
+      return status;
+    }
+  }
   if (status == MOFFT_SUCCESS && diagnostics) {
     diagnostics->used_wisdom = wisdom != 0;
     diagnostics->used_model_fallback = wisdom == 0;

@@ -149,3 +149,32 @@ def test_host_buffers_distance_and_stream():
         got = o.cpu().numpy()
     assert rel_l2(got[:, :N], want) <= TOL[m.FORM_TF32X3]
     assert not np.any(got[:, N:])           # padding between transforms untouched
+
+
+def test_form_from_plan_option_flags():
+    import ctypes
+    import torch
+    lib = m.load()
+    x = _mix(4, seed=12)
+    want = _expected(x, m.FORWARD)
+    for bit, form in ((m.PLAN_FORM_TF32X3, m.FORM_TF32X3), (m.PLAN_FORM_BF16X3, m.FORM_BF16X3)):
+        h = ctypes.c_void_p()
+        opts = m.PlanOptions(m.PLANNER_PRETUNED, bit, 0, 0)
+        diag = m.Diagnostics()
+        st = lib.mofft_plan_create_batched_f32(ctypes.byref(h), N, 4, 0, m.FORWARD,
+                                               m.OUT_OF_PLACE, ctypes.byref(opts),
+                                               ctypes.byref(diag))
+        assert st == m.Status.SUCCESS
+        plan = m.Plan(h.value, 32)
+        assert plan.precision_form == form
+        d = torch.from_numpy(x).cuda()
+        out = torch.empty_like(d)
+        plan.execute(d, out)
+        plan.destroy()
+        assert rel_l2(out.cpu().numpy(), want) <= TOL[form]
+    # a length without a tensor-core kernel
+    h = ctypes.c_void_p()
+    opts = m.PlanOptions(m.PLANNER_PRETUNED, m.PLAN_FORM_TF32X3, 0, 0)
+    st = lib.mofft_plan_create_with_options_f32(ctypes.byref(h), 2048, m.FORWARD,
+                                                m.OUT_OF_PLACE, ctypes.byref(opts), None)
+    assert st == m.Status.UNSUPPORTED_SIZE and h.value is None

@@ -63,6 +63,8 @@ def test_options_validation_before_hardware():
     bad = [m.PlanOptions(m.PLANNER_MEASURE, 1, 0, 0),     # MEASURE with flags
            m.PlanOptions(7, 0, 0, 0),                     # bad mode
            m.PlanOptions(0, 4, 0, 0),                     # unknown flag
+           m.PlanOptions(0, m.PLAN_FORM_TF32X3 | m.PLAN_FORM_BF16X3, 0, 0),  # two forms
+           m.PlanOptions(m.PLANNER_MEASURE, m.PLAN_FORM_TF32X3, 0, 0),      # MEASURE + form
            m.PlanOptions(m.PLANNER_MEASURE, 0, 65, 0),    # > 64 candidates
            m.PlanOptions(m.PLANNER_MEASURE, 0, 0, 32)]    # > 31 samples
     for opts in bad:
@@ -71,6 +73,12 @@ def test_options_validation_before_hardware():
                                                      ctypes.byref(diag))
         assert st == m.Status.INVALID_ARGUMENT
         assert h.value is None
+    # a precision form is an FP32 option
+    form = m.PlanOptions(0, m.PLAN_FORM_BF16X3, 0, 0)
+    st = lib.mofft_plan_create_with_options_f64(ctypes.byref(h), 4096, m.FORWARD,
+                                                 m.OUT_OF_PLACE, ctypes.byref(form),
+                                                 ctypes.byref(diag))
+    assert st == m.Status.INVALID_ARGUMENT and h.value is None
     st = lib.mofft_plan_create_f32(None, 64, m.FORWARD, m.OUT_OF_PLACE)
     assert st == m.Status.INVALID_ARGUMENT
     st = lib.mofft_plan_create_f64(ctypes.byref(h), 64, 0, m.OUT_OF_PLACE)
