@@ -393,6 +393,32 @@ int mofft_group_chain_preferred(int precision_bits, unsigned bank,
   int found = 0;
   mofft_schedule cand;
   group_score score;
+  /* A tuned list of two or more kernels fixes the pass count and each pass's
+   * kernel (the autotuner measured that schedule, e.g. three narrow passes
+   * where two wide ones exist); without a matching split, group canonically. */
+  int npref = 0;
+  while (preferred && npref < MOFFT_MAX_PASSES && preferred[npref] >= 0) ++npref;
+  if (npref >= 2 && npref <= count) {
+    int cuts[MOFFT_MAX_PASSES];
+    for (int i = 0; i < npref - 1; ++i) cuts[i] = i + 1;
+    for (;;) {
+      if (try_split(precision_bits, bank, chain, count, cuts, npref, total,
+                    preferred, &cand, &score)) {
+        int match = 1;
+        for (int p = 0; p < npref; ++p)
+          if (cand.pass[p].kernel != preferred[p]) match = 0;
+        if (match) {
+          *best = cand;
+          return 1;
+        }
+      }
+      int i = npref - 2;
+      while (i >= 0 && cuts[i] == count - (npref - 1 - i)) --i;
+      if (i < 0) break;
+      ++cuts[i];
+      for (int k = i + 1; k < npref - 1; ++k) cuts[k] = cuts[k - 1] + 1;
+    }
+  }
   for (int passes = 1; passes <= MOFFT_MAX_PASSES && passes <= count; ++passes) {
     int cuts[MOFFT_MAX_PASSES];
     /* enumerate increasing cut positions in [1, count-1] */

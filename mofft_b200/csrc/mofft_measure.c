@@ -154,6 +154,46 @@ static int enumerate(int precision_bits, size_t length, candidate *pool,
         add_candidate(pool, &count, capacity, &c);
     }
   }
+  /* three-pass splits of narrow column kernels (lines of 64..512 points,
+   * whose tiles span 16 or more adjacent columns): more passes, but longer
+   * contiguous runs in the strided passes */
+  for (int i = 0; i < n; ++i) {
+    const mofft_kernel_desc *a = mofft_cuda_kernel_get(i);
+    if (a->kind != MOFFT_KERNEL_COLS || a->precision_bits != precision_bits ||
+        a->length < 64 || a->length > 512 || length % (size_t)a->length != 0)
+      continue;
+    for (int j = 0; j < n; ++j) {
+      const mofft_kernel_desc *b = mofft_cuda_kernel_get(j);
+      if (b->kind != MOFFT_KERNEL_COLS || b->precision_bits != precision_bits ||
+          b->length < 64 || b->length > 512 ||
+          (length / (size_t)a->length) % (size_t)b->length != 0)
+        continue;
+      const size_t rest = length / (size_t)a->length / (size_t)b->length;
+      for (int k = 0; k < n; ++k) {
+        const mofft_kernel_desc *d = mofft_cuda_kernel_get(k);
+        if (d->kind != MOFFT_KERNEL_COLS || d->precision_bits != precision_bits ||
+            d->length < 64 || d->length > 512 || (size_t)d->length != rest)
+          continue;
+        memset(&c, 0, sizeof(c));
+        no_preference(&c);
+        c.preferred[0] = i;
+        c.preferred[1] = j;
+        c.preferred[2] = k;
+        c.bank = 0;
+        memcpy(c.chain, a->radices, (size_t)a->radix_count * sizeof(int));
+        memcpy(c.chain + a->radix_count, b->radices, (size_t)b->radix_count * sizeof(int));
+        memcpy(c.chain + a->radix_count + b->radix_count, d->radices,
+               (size_t)d->radix_count * sizeof(int));
+        c.count = a->radix_count + b->radix_count + d->radix_count;
+        mofft_schedule s;
+        if (mofft_group_chain_preferred(precision_bits, 0, c.chain, c.count,
+                                        (long long)length, c.preferred, &s) &&
+            s.pass_count == 3 && s.pass[0].kernel == i && s.pass[1].kernel == j &&
+            s.pass[2].kernel == k)
+          add_candidate(pool, &count, capacity, &c);
+      }
+    }
+  }
   /* the generic family with its default chain */
   memset(&c, 0, sizeof(c));
   no_preference(&c);
