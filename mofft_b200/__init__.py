@@ -55,7 +55,7 @@ STAGE_LAYOUT_SECTION = 1
 TRANSPOSE_LINEAR = 0
 TRANSPOSE_BLOCKED = 1
 MAX_PLAN_DEPTH = 64
-KERNEL_ROWS, KERNEL_COLS, KERNEL_GENERIC, KERNEL_TENSOR = 0, 1, 2, 3
+KERNEL_ROWS, KERNEL_COLS, KERNEL_GENERIC, KERNEL_TENSOR, KERNEL_TENSOR_COLS = 0, 1, 2, 3, 4
 
 
 class MofftError(RuntimeError):

@@ -595,6 +595,10 @@ void mofft_core_destroy(mofft_core *c) {
 
 static size_t align256(size_t x) { return (x + 255u) & ~(size_t)255u; }
 
+static int is_tensor_kind(int kind) {
+  return kind == MOFFT_KERNEL_TENSOR || kind == MOFFT_KERNEL_TENSOR_COLS;
+}
+
 /* Build device state (twiddles, workspace) for c->sched. */
 static mofft_status materialise_schedule(mofft_core *c) {
   const size_t cb = mofft_complex_bytes(c->precision_bits);
@@ -617,7 +621,7 @@ static mofft_status materialise_schedule(mofft_core *c) {
       bytes = align256(bytes + lo_n * cb);
     }
     ps->aux_offset = ps->status_offset = 0;
-    if (ps->kind == MOFFT_KERNEL_TENSOR) {
+    if (is_tensor_kind(ps->kind)) {
       ps->aux_offset = bytes;
       bytes = align256(bytes + mofft_cuda_tensor_aux_bytes(mofft_cuda_kernel_get(ps->kernel)->form));
       ps->status_offset = bytes;
@@ -638,7 +642,7 @@ static mofft_status materialise_schedule(mofft_core *c) {
       mofft_write_twiddles(host + ps->tw_hi_offset, c->precision_bits, m, 0, lo_n, hi_n);
       mofft_write_twiddles(host + ps->tw_lo_offset, c->precision_bits, m, 0, 1, lo_n);
     }
-    if (ps->kind == MOFFT_KERNEL_TENSOR) {
+    if (is_tensor_kind(ps->kind)) {
       double fr[256], fi[256];
       for (int k = 0; k < 16; ++k)
         for (int r = 0; r < 16; ++r) {
@@ -696,35 +700,50 @@ static int chain_from_factors(const mofft_core *c, int *chain) {
   return c->depth;
 }
 
-/* (Re)build the GPU schedule from c->factors and c->kernel_bank. */
-static int tensor_kernel_index(int form) {
+static int tensor_kernel_index(int kind, int form) {
   const int n = mofft_cuda_kernel_count();
   for (int i = 0; i < n; ++i) {
     const mofft_kernel_desc *d = mofft_cuda_kernel_get(i);
-    if (d->kind == MOFFT_KERNEL_TENSOR && d->form == form) return i;
+    if (d->kind == kind && d->form == form) return i;
   }
   return -1;
 }
 
-/* One-pass schedule of the tensor-core kernel of c->form. */
+/* Schedule of the tensor-core kernels of c->form: one pass of the whole-
+ * transform kernel when it has c->length, else two passes of the column
+ * kernel when c->length is the square of its line length. */
 static mofft_status build_tensor_schedule(mofft_core *c) {
-  const int k = tensor_kernel_index(c->form);
-  if (k < 0) return MOFFT_UNSUPPORTED_SIZE;
-  const mofft_kernel_desc *d = mofft_cuda_kernel_get(k);
-  if (c->precision_bits != d->precision_bits || c->length != (size_t)d->length)
-    return MOFFT_UNSUPPORTED_SIZE;
   mofft_schedule sched;
   memset(&sched, 0, sizeof(sched));
-  sched.pass_count = 1;
-  mofft_pass *ps = &sched.pass[0];
-  ps->kernel = k;
-  ps->kind = MOFFT_KERNEL_TENSOR;
-  ps->length = d->length;
-  ps->lines = d->lines;
-  ps->radix_count = d->radix_count;
-  memcpy(ps->radices, d->radices, (size_t)d->radix_count * sizeof(int));
-  ps->ns_outer = 1;
-  ps->smem_bytes = d->smem_bytes;
+  int k = tensor_kernel_index(MOFFT_KERNEL_TENSOR, c->form);
+  const mofft_kernel_desc *d = k >= 0 ? mofft_cuda_kernel_get(k) : NULL;
+  int passes = 0, kind = MOFFT_KERNEL_TENSOR;
+  if (d && c->precision_bits == d->precision_bits && c->length == (size_t)d->length) {
+    passes = 1;
+  } else {
+    k = tensor_kernel_index(MOFFT_KERNEL_TENSOR_COLS, c->form);
+    d = k >= 0 ? mofft_cuda_kernel_get(k) : NULL;
+    if (d && c->precision_bits == d->precision_bits &&
+        c->length == (size_t)d->length * (size_t)d->length) {
+      passes = 2;
+      kind = MOFFT_KERNEL_TENSOR_COLS;
+    }
+  }
+  if (passes == 0) return MOFFT_UNSUPPORTED_SIZE;
+  sched.pass_count = passes;
+  long long ns = 1;
+  for (int p = 0; p < passes; ++p) {
+    mofft_pass *ps = &sched.pass[p];
+    ps->kernel = k;
+    ps->kind = kind;
+    ps->length = d->length;
+    ps->lines = d->lines;
+    ps->radix_count = d->radix_count;
+    memcpy(ps->radices, d->radices, (size_t)d->radix_count * sizeof(int));
+    ps->ns_outer = ns;
+    ps->smem_bytes = d->smem_bytes;
+    ns *= d->length;
+  }
   c->sched = sched;
   return materialise_schedule(c);
 }
@@ -732,7 +751,7 @@ static mofft_status build_tensor_schedule(mofft_core *c) {
 mofft_status mofft_core_check_status(const mofft_core *c) {
   for (int p = 0; p < c->sched.pass_count; ++p) {
     const mofft_pass *ps = &c->sched.pass[p];
-    if (ps->kind != MOFFT_KERNEL_TENSOR) continue;
+    if (!is_tensor_kind(ps->kind)) continue;
     int word = 0;
     if (cudaMemcpy(&word, (const unsigned char *)c->d_twiddles + ps->status_offset,
                    sizeof(word), cudaMemcpyDeviceToHost) != cudaSuccess) {
@@ -744,6 +763,7 @@ mofft_status mofft_core_check_status(const mofft_core *c) {
   return MOFFT_SUCCESS;
 }
 
+/* (Re)build the GPU schedule from c->factors, c->kernel_bank and c->form. */
 mofft_status mofft_core_build(mofft_core *c) {
   if (c->form != 0) return build_tensor_schedule(c);
   int chain[MOFFT_MAX_STAGES];
@@ -872,7 +892,7 @@ mofft_status mofft_core_enqueue(const mofft_core *c, const void *in, void *out,
     a.split_shift = ps->split_shift;
     a.conj_in = backward && p == 0;
     a.conj_out = backward && p == P - 1;
-    if (ps->kind == MOFFT_KERNEL_TENSOR) {
+    if (is_tensor_kind(ps->kind)) {
       a.aux = (const unsigned char *)c->d_twiddles + ps->aux_offset;
       a.status = (int *)((unsigned char *)c->d_twiddles + ps->status_offset);
     }
@@ -1029,7 +1049,7 @@ mofft_status mofft_core_enqueue_indirect(const mofft_core *c, const void *const 
   if (P > 2 || batch <= 0) return MOFFT_UNSUPPORTED_SIZE;
   for (int p = 0; p < P; ++p)
     if (c->sched.pass[p].kind == MOFFT_KERNEL_GENERIC ||
-        c->sched.pass[p].kind == MOFFT_KERNEL_TENSOR)
+        is_tensor_kind(c->sched.pass[p].kind))
       return MOFFT_UNSUPPORTED_SIZE;
   const int backward = c->direction == MOFFT_BACKWARD;
   for (int p = 0; p < P; ++p) {

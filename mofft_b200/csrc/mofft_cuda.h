@@ -19,8 +19,10 @@ typedef enum {
   MOFFT_KERNEL_ROWS = 0,    /* single pass, whole transforms per CTA */
   MOFFT_KERNEL_COLS = 1,    /* one pass of a multi-pass transform */
   MOFFT_KERNEL_GENERIC = 2, /* runtime stage list, ROWS or COLS addressing */
-  MOFFT_KERNEL_TENSOR = 3   /* whole transforms per CTA, DFT-matrix stages on
+  MOFFT_KERNEL_TENSOR = 3,  /* whole transforms per CTA, DFT-matrix stages on
                                the tensor cores (a precision form) */
+  MOFFT_KERNEL_TENSOR_COLS = 4  /* one column pass of a multi-pass transform,
+                                   DFT-matrix stages on the tensor cores */
 } mofft_kernel_kind;
 
 typedef struct {

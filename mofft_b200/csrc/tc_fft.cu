@@ -573,6 +573,308 @@ struct TcInst {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Column passes on the tensor cores: one pass of a four-step transform whose
+// lines have 256 = 16 x 16 points (n = 65536 runs two of them).  A tile is 16
+// adjacent lines of one batch entry; its 256 butterflies per stage (16 per
+// line) are the 256 rows of the same GEMMs as above.  Thread j owns line
+// c = j mod 16 and butterfly bb = j / 16, so that consecutive threads read
+// consecutive lines: every global access is a 16-element (128-byte) run.
+// Pass with Ns = 1: outputs are staged in shared memory and the tile (16
+// whole lines, contiguous) is written with coalesced stores; pass with
+// Ns > 1: the super-stage twiddle W_{Ns 256}^{(line mod Ns) i} is applied on
+// load from the two-level table and outputs go to y[line + k Ns].
+// ---------------------------------------------------------------------------
+constexpr int kColsL = 256;
+constexpr int kColsC = 16;
+constexpr int kColsPitch = kColsL + kColsL / 32 + 1;   // padded words per line
+
+template <int FORM>
+struct ColsPlan {
+  using F = FormTraits<FORM>;
+  static constexpr int kBHalf = Plan<FORM>::kBHalf;
+  static constexpr int kData = 2 * kColsC * kColsPitch * 4;
+  static constexpr int kOffB = 0;
+  static constexpr int kOffData = kOffB + 2 * kBHalf;
+  static constexpr int kOffBar = (kOffData + kData + 15) & ~15;
+  static constexpr int kOffTmem = kOffBar + 16;
+  static constexpr int kBytes = kOffTmem + 16 + 1024;
+};
+
+struct TcColsArgs {
+  const float2 *in;
+  float2 *out;
+  const float2 *tw;          // stage table of the 256-point line [16, 16]
+  const float2 *tw_hi;       // super-stage twiddle, two-level table
+  const float2 *tw_lo;
+  const unsigned char *bmat;
+  int *status;
+  long long batch;
+  long long in_dist;
+  long long out_dist;
+  long long total;           // transform length M
+  long long ns;              // Ns of this pass (1 or a multiple of 16)
+  int split_shift;
+  float sign_in;
+  float sign_out;
+};
+
+__device__ __forceinline__ int cpad(int i) { return i + (i >> 5); }
+
+template <int FORM>
+__global__ void __launch_bounds__(kThreads, FormTraits<FORM>::kMinBlocks)
+    tc_cols256_kernel(const TcColsArgs a) {
+  using P = ColsPlan<FORM>;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char *base = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char *b_tiles = base + P::kOffB;
+  float *sre = reinterpret_cast<float *>(base + P::kOffData);
+  float *sim = sre + kColsC * kColsPitch;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(base + P::kOffBar);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(base + P::kOffTmem);
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const uint32_t mma_bar = smem_u32(&bars[0]);
+
+  for (int i = tid; i < 2 * P::kBHalf / 16; i += kThreads)
+    reinterpret_cast<uint4 *>(b_tiles)[i] = __ldg(reinterpret_cast<const uint4 *>(a.bmat) + i);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mma_bar), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(FormTraits<FORM>::kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  const int j = tid;
+  const int c = j & (kColsC - 1);   // line within the tile
+  const int bb = j >> 4;            // butterfly within the line
+  const int tile_row = j >> 7;
+  const uint32_t lane_off = (uint32_t)(32 * (warp & 3)) << 16;
+  const uint32_t t_d = tmem + lane_off + Plan<FORM>::kColD + 32u * tile_row;
+  const uint32_t t_hi =
+      tmem + lane_off + Plan<FORM>::kColAHi + (uint32_t)(FormTraits<FORM>::kACols * tile_row);
+  const uint32_t t_lo =
+      tmem + lane_off + Plan<FORM>::kColALo + (uint32_t)(FormTraits<FORM>::kACols * tile_row);
+  const uint32_t b_hi = smem_u32(b_tiles);
+  const uint32_t b_lo = b_hi + P::kBHalf;
+  const long long lines_total = a.total / kColsL;
+  const long long groups = lines_total / kColsC;
+  const long long tiles = a.batch * groups;
+  const long long mask = (1LL << a.split_shift) - 1;
+
+  bool failed = false;
+  int mma_pending = 0;
+  uint32_t mma_phase = 0;
+#pragma unroll 1
+  for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const long long b = tile / groups;
+    const long long line0 = (tile - b * groups) * kColsC;
+    const long long line = line0 + c;
+    const long long jq = line / a.ns;
+    const long long jm = line - jq * a.ns;
+    const float2 *gin = a.in + b * a.in_dist + line;
+    float2 *out_b = a.out + b * a.out_dist;
+#pragma unroll 1
+    for (int stage = 0; stage < 2; ++stage) {
+      float v[32];
+      if (stage == 0) {
+#pragma unroll
+        for (int r = 0; r < kR; ++r) {
+          const int i = bb + 16 * r;
+          const float2 x = __ldcg(gin + (long long)i * lines_total);
+          float re = x.x, im = x.y * a.sign_in;
+          if (jm != 0 && i != 0) {
+            const long long e = jm * (long long)i;
+            const float2 hi = __ldg(a.tw_hi + (e >> a.split_shift));
+            const float2 lo = __ldg(a.tw_lo + (e & mask));
+            float wr = hi.x, wi = hi.y;
+            cmul<float>(wr, wi, lo.x, lo.y);
+            cmul<float>(re, im, wr, wi);
+          }
+          v[r] = re;
+          v[16 + r] = im;
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < kR; ++r) {
+          v[r] = sre[c * kColsPitch + cpad(bb + 16 * r)];
+          v[16 + r] = sim[c * kColsPitch + cpad(bb + 16 * r)];
+        }
+        twiddle16(v, a.tw + bb, 16);   // W_256^{bb r}
+      }
+      store_split<FORM>(t_hi, t_lo, v);
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        issue_mmas<FORM>(tmem, b_hi, b_lo);
+        asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                mma_bar)
+            : "memory");
+      }
+      mma_pending = 1;
+      const bool ok = mbar_wait(mma_bar, mma_phase);
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        break;
+      }
+      mma_phase ^= 1u;
+      mma_pending = 0;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      uint32_t d[32];
+      tmem_ld32(t_d, d);
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      if (stage == 0 || a.ns == 1) {
+        // line outputs at 16 bb + k (stage 0) or bb + 16 k (stage 1)
+#pragma unroll
+        for (int k = 0; k < kR; ++k) {
+          const int idx = stage == 0 ? 16 * bb + k : bb + 16 * k;
+          sre[c * kColsPitch + cpad(idx)] = __uint_as_float(d[k]);
+          sim[c * kColsPitch + cpad(idx)] = __uint_as_float(d[16 + k]);
+        }
+        __syncthreads();
+        if (stage == 1) {
+          // 16 whole lines, contiguous in the output: coalesced stores
+          float2 *dst = out_b + line0 * kColsL;
+#pragma unroll
+          for (int q = 0; q < kColsC * kColsL / kThreads; ++q) {
+            const int e = tid + q * kThreads;
+            const int cc = e / kColsL;
+            const int k = e - cc * kColsL;
+            float2 o;
+            o.x = sre[cc * kColsPitch + cpad(k)];
+            o.y = sim[cc * kColsPitch + cpad(k)] * a.sign_out;
+            __stcs(dst + e, o);
+          }
+          __syncthreads();
+        }
+      } else {
+        // y[(line / Ns) Ns 256 + line mod Ns + k' Ns], k' = bb + 16 k
+        float2 *dst = out_b + jq * a.ns * kColsL + jm;
+#pragma unroll
+        for (int k = 0; k < kR; ++k) {
+          float2 o;
+          o.x = __uint_as_float(d[k]);
+          o.y = __uint_as_float(d[16 + k]) * a.sign_out;
+          __stcs(dst + (long long)(bb + 16 * k) * a.ns, o);
+        }
+        __syncthreads();
+      }
+    }
+    if (failed) break;
+  }
+  if (failed && tid == 0) {
+    atomicExch(a.status, 1);
+    if (mma_pending) (void)mbar_wait(mma_bar, mma_phase);
+  }
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(FormTraits<FORM>::kTmemCols)
+                 : "memory");
+  }
+}
+
+template <int FORM>
+struct TcColsInst {
+  static constexpr size_t smem() { return (size_t)ColsPlan<FORM>::kBytes; }
+  static const void *func() {
+    return reinterpret_cast<const void *>(&tc_cols256_kernel<FORM>);
+  }
+  static int persistent_grid() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    if (cached[dev] > 0) return cached[dev];
+    cudaFuncAttributes fa;
+    int sms = 0, regs_sm = 0, smem_sm = 0, reserved = 0, threads_sm = 0;
+    if (cudaFuncGetAttributes(&fa, tc_cols256_kernel<FORM>) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev) !=
+            cudaSuccess)
+      return 0;
+    const int warp_regs = ((fa.numRegs * 32 + 255) / 256) * 256;
+    int per_sm = regs_sm / (warp_regs * (kThreads / 32));
+    const int by_smem = smem_sm / ((int)smem() + reserved);
+    const int by_threads = threads_sm / kThreads;
+    const int by_tmem = 512 / FormTraits<FORM>::kTmemCols;
+    if (by_smem < per_sm) per_sm = by_smem;
+    if (by_threads < per_sm) per_sm = by_threads;
+    if (by_tmem < per_sm) per_sm = by_tmem;
+    if (per_sm < 1) per_sm = 1;
+    cached[dev] = per_sm * sms;
+    return cached[dev];
+  }
+  static cudaError_t launch(const mofft_pass_args *p, cudaStream_t s) {
+    if (p->in_table || p->out_table) return cudaErrorNotSupported;
+    if (!p->aux || !p->status) return cudaErrorInvalidValue;
+    if (p->total % kColsL != 0 || (p->total / kColsL) % kColsC != 0) return cudaErrorInvalidValue;
+    if (p->ns_outer != 1 && p->ns_outer % kColsC != 0) return cudaErrorInvalidValue;
+    if (p->ns_outer > 1 && (p->split_shift < 0 || p->split_shift > 40))
+      return cudaErrorInvalidValue;
+    const long long tiles = p->batch * ((p->total / kColsL) / kColsC);
+    if (tiles <= 0) return cudaSuccess;
+    const int resident = persistent_grid();
+    if (resident <= 0) return cudaErrorInvalidConfiguration;
+    TcColsArgs a;
+    a.in = static_cast<const float2 *>(p->in);
+    a.out = static_cast<float2 *>(p->out);
+    a.tw = static_cast<const float2 *>(p->tw);
+    a.tw_hi = static_cast<const float2 *>(p->tw_hi);
+    a.tw_lo = static_cast<const float2 *>(p->tw_lo);
+    a.bmat = static_cast<const unsigned char *>(p->aux);
+    a.status = p->status;
+    a.batch = p->batch;
+    a.in_dist = p->in_dist;
+    a.out_dist = p->out_dist;
+    a.total = p->total;
+    a.ns = p->ns_outer;
+    a.split_shift = p->ns_outer > 1 ? p->split_shift : 0;
+    a.sign_in = p->conj_in ? -1.0f : 1.0f;
+    a.sign_out = p->conj_out ? -1.0f : 1.0f;
+    const long long grid = tiles < resident ? tiles : resident;
+    tc_cols256_kernel<FORM><<<(unsigned)grid, kThreads, smem(), s>>>(a);
+    return cudaGetLastError();
+  }
+  static Entry entry(const char *name) {
+    Entry e{};
+    e.desc.name = name;
+    e.desc.precision_bits = 32;
+    e.desc.kind = MOFFT_KERNEL_TENSOR_COLS;
+    e.desc.length = kColsL;
+    e.desc.lines = kColsC;
+    e.desc.threads = kThreads;
+    e.desc.staged = 0;
+    e.desc.radix_count = 2;
+    for (int i = 0; i < 8; ++i) e.desc.radices[i] = i < 2 ? kR : 0;
+    e.desc.smem_bytes = smem();
+    e.desc.form = FORM;
+    e.launch = &launch;
+    e.func = &func;
+    return e;
+  }
+};
+
 // ---- host side: the B operand tables ------------------------------------
 
 static uint32_t host_f32_bits(float x) {
@@ -612,6 +914,8 @@ const Entry *entries_tensor(int *n) {
   static const Entry e[] = {
       tc::TcInst<kFormTf32x3>::entry("tensor_float_4096_tf32x3_r16x3"),
       tc::TcInst<kFormBf16x3>::entry("tensor_float_4096_bf16x3_r16x3"),
+      tc::TcColsInst<kFormTf32x3>::entry("tensor_cols_float_256_tf32x3_c16"),
+      tc::TcColsInst<kFormBf16x3>::entry("tensor_cols_float_256_bf16x3_c16"),
   };
   *n = (int)(sizeof(e) / sizeof(e[0]));
   return e;

@@ -1,4 +1,4 @@
-"""Tensor-core precision forms of the n = 4096 FP32 transform.
+"""Tensor-core precision forms of the FP32 transform (n = 4096 and 65536).
 
 MOFFT_FORM_TF32X3 and MOFFT_FORM_BF16X3 run the three radix-16 Stockham
 stages as DFT-matrix GEMMs on the tcgen05 tensor cores with split operands
@@ -6,6 +6,9 @@ stages as DFT-matrix GEMMs on the tcgen05 tensor cores with split operands
 long-double oracle on the precision-mix inputs (a third uniform[-1,1), a
 third log-uniform magnitudes 1e-3..1e3 with uniform phase, a third single
 tones), forward and backward, in place and out of place, through the C-ABI.
+n = 65536 runs two column passes of 256-point lines (same GEMMs, 16 lines
+per tile, super-stage twiddles between the passes); its bounds are the same
+per stage, four stages instead of three.
 
 Tolerances (relative L2 error over the batch, written here because the forms
 are not FP32-exact):
@@ -33,8 +36,8 @@ TOL = {m.FORM_TF32X3: 4e-6, m.FORM_BF16X3: 1e-4}
 NAMES = {m.FORM_TF32X3: "tf32x3", m.FORM_BF16X3: "bf16x3"}
 
 
-def _mix(batch: int, seed: int = 3) -> np.ndarray:
-    return workloads.precision_mix(batch * N, N, seed=seed)
+def _mix(batch: int, seed: int = 3, n: int = N) -> np.ndarray:
+    return workloads.precision_mix(batch * n, n, seed=seed)
 
 
 def _expected(x: np.ndarray, direction: int) -> np.ndarray:
@@ -43,10 +46,10 @@ def _expected(x: np.ndarray, direction: int) -> np.ndarray:
 
 def _run(x: np.ndarray, direction: int, placement: int, form: int) -> np.ndarray:
     import torch
-    batch = x.shape[0]
+    batch, n = x.shape
     d = torch.from_numpy(x).cuda()
     out = d if placement == m.IN_PLACE else torch.empty_like(d)
-    with m.Plan.create(N, direction, placement, bits=32, batch=batch) as plan:
+    with m.Plan.create(n, direction, placement, bits=32, batch=batch) as plan:
         plan.set_precision_form(form)
         assert plan.precision_form == form
         plan.execute(d, out)
@@ -178,3 +181,38 @@ def test_form_from_plan_option_flags():
     st = lib.mofft_plan_create_with_options_f32(ctypes.byref(h), 2048, m.FORWARD,
                                                 m.OUT_OF_PLACE, ctypes.byref(opts), None)
     assert st == m.Status.UNSUPPORTED_SIZE and h.value is None
+
+
+N2 = 65536
+TOL2 = {m.FORM_TF32X3: 6e-6, m.FORM_BF16X3: 1.5e-4}
+
+
+@pytest.mark.parametrize("form", [m.FORM_TF32X3, m.FORM_BF16X3])
+@pytest.mark.parametrize("direction", [m.FORWARD, m.BACKWARD])
+@pytest.mark.parametrize("placement", [m.OUT_OF_PLACE, m.IN_PLACE])
+def test_form_65536_matches_oracle(form, direction, placement):
+    x = _mix(6, seed=5, n=N2)
+    want = _expected(x, direction)
+    got = _run(x, direction, placement, form)
+    err = rel_l2(got, want)
+    assert err <= TOL2[form], (NAMES[form], direction, placement, err)
+    for lo, hi in ((0, 2), (2, 4), (4, 6)):   # each input class of the mix
+        assert rel_l2(got[lo:hi], want[lo:hi]) <= TOL2[form]
+
+
+def test_form_65536_schedule_and_error_ordering():
+    kernels = {k["index"]: k for k in m.kernels()}
+    with m.Plan.create(N2, m.FORWARD, m.OUT_OF_PLACE, bits=32, batch=2) as plan:
+        plan.set_precision_form(m.FORM_TF32X3)
+        s = plan.schedule()
+        assert s["pass_count"] == 2
+        assert [kernels[k]["name"] for k in s["kernels"]] == \
+            ["tensor_cols_float_256_tf32x3_c16"] * 2
+    x = _mix(3, seed=6, n=N2)
+    want = _expected(x, m.FORWARD)
+    errs = {f: rel_l2(_run(x, m.FORWARD, m.OUT_OF_PLACE, f), want)
+            for f in (m.FORM_FP32, m.FORM_TF32X3, m.FORM_BF16X3)}
+    print("n=65536 rel-L2 vs oracle:", {("fp32", "tf32x3", "bf16x3")[f]: f"{e:.3e}"
+                                        for f, e in errs.items()})
+    assert errs[m.FORM_FP32] <= fp32_tol(N2)
+    assert errs[m.FORM_TF32X3] < errs[m.FORM_BF16X3]

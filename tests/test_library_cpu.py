@@ -202,10 +202,17 @@ def test_tensor_forms_registered_and_never_planned():
                     for k in ks if k["kind"] == m.KERNEL_TENSOR)
     assert tensor == [("tensor_float_4096_bf16x3_r16x3", 4096, [16, 16, 16], 32),
                       ("tensor_float_4096_tf32x3_r16x3", 4096, [16, 16, 16], 32)]
+    cols = sorted((k["name"], k["length"], k["lines"], k["radices"])
+                  for k in ks if k["kind"] == m.KERNEL_TENSOR_COLS)
+    assert cols == [("tensor_cols_float_256_bf16x3_c16", 256, 16, [16, 16]),
+                    ("tensor_cols_float_256_tf32x3_c16", 256, 16, [16, 16])]
     # the planner keeps FP32 (CUDA-core) kernels unless a form is requested
     for bits in (32, 64):
         s = m.schedule_preview(4096, bits)
-        assert all(ks[k]["kind"] != m.KERNEL_TENSOR for k in s["kernels"])
+        assert all(ks[k]["kind"] not in (m.KERNEL_TENSOR, m.KERNEL_TENSOR_COLS)
+                   for k in s["kernels"])
+    s = m.schedule_preview(65536, 32)
+    assert all(ks[k]["kind"] == m.KERNEL_COLS for k in s["kernels"])
 
 
 def test_mixed_lengths_use_specialised_kernels():
