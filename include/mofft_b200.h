@@ -135,14 +135,15 @@ mofft_status mofft_execute_fixed_scratch_f32(const mofft_complex_f32 *input,
  * transforms run in the plan's own precision on the CPU cores).
  *
  *   MOFFT_FORM_FP32    FP32 butterflies on the CUDA cores (the default).
- *   MOFFT_FORM_TF32X3  the three radix-16 stages of n = 4096 as DFT-matrix
+ *   MOFFT_FORM_TF32X3  the radix-16 stages (three for n = 4096, four in two
+ *                      column passes for n = 65536) as DFT-matrix
  *                      GEMMs on the tensor cores; every operand x is split
  *                      into TF32 terms hi + lo and each product is
  *                      lo*hi + hi*lo + hi*hi, accumulated in FP32 (about 21
  *                      significant bits per product).
  *   MOFFT_FORM_BF16X3  the same with BF16 terms (about 16 bits).
  *
- * Tensor-core forms exist for FP32 plans of length 4096 only (other lengths:
+ * Tensor-core forms exist for FP32 plans of length 4096 and 65536 (others:
  * MOFFT_UNSUPPORTED_SIZE, the plan keeps its form); they run direct batches
  * (not the serving engine's pointer tables).  Twiddle multiplications and
  * the shuffles between stages stay FP32 on the CUDA cores.  The kernel bounds
