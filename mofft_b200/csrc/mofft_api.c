@@ -857,23 +857,32 @@ static int is_device_pointer(const void *p) {
 /* Enqueue the plan's passes: in -> out on `stream` (device pointers). */
 mofft_status mofft_core_enqueue(const mofft_core *c, const void *in, void *out,
                                 void *stream) {
+  return mofft_core_enqueue_batch(c, in, out, c->batch, c->distance, stream);
+}
+
+/* The same for `batch` transforms `distance` elements apart (a plan made for
+ * one transform serving a request of many).  A schedule that routes through
+ * the plan's workspace needs batch <= the plan's batch. */
+mofft_status mofft_core_enqueue_batch(const mofft_core *c, const void *in, void *out,
+                                      size_t batch, size_t distance, void *stream) {
   const size_t cb = mofft_complex_bytes(c->precision_bits);
   const int P = c->sched.pass_count;
   const int backward = c->direction == MOFFT_BACKWARD;
   const void *src = in;
-  long long src_dist = (long long)c->distance;
+  if (distance < c->length) return MOFFT_INVALID_ARGUMENT;
+  long long src_dist = (long long)distance;
   for (int p = 0; p < P; ++p) {
     const mofft_pass *ps = &c->sched.pass[p];
     void *dst;
     long long dst_dist;
     if (p == P - 1) {
       dst = out;
-      dst_dist = (long long)c->distance;
+      dst_dist = (long long)distance;
     } else if (src != out) {
       dst = out;
-      dst_dist = (long long)c->distance;
+      dst_dist = (long long)distance;
     } else {
-      if (!c->d_work) return MOFFT_INTERNAL_ERROR;
+      if (!c->d_work || batch > c->batch) return MOFFT_INTERNAL_ERROR;
       dst = c->d_work;
       dst_dist = (long long)c->length;
     }
@@ -884,7 +893,7 @@ mofft_status mofft_core_enqueue(const mofft_core *c, const void *in, void *out,
     a.tw = (const unsigned char *)c->d_twiddles + ps->tw_offset;
     a.tw_hi = (const unsigned char *)c->d_twiddles + ps->tw_hi_offset;
     a.tw_lo = (const unsigned char *)c->d_twiddles + ps->tw_lo_offset;
-    a.batch = (long long)c->batch;
+    a.batch = (long long)batch;
     a.in_dist = src_dist;
     a.out_dist = dst_dist;
     a.total = (long long)c->length;

@@ -45,6 +45,8 @@ mofft_status mofft_core_check_status(const mofft_core *c);
 void mofft_core_destroy(mofft_core *c);
 mofft_status mofft_core_enqueue(const mofft_core *c, const void *in, void *out,
                                 void *stream);
+mofft_status mofft_core_enqueue_batch(const mofft_core *c, const void *in, void *out,
+                                      size_t batch, size_t distance, void *stream);
 mofft_status mofft_core_execute(const mofft_core *c, const void *in, void *out);
 mofft_status mofft_core_enqueue_indirect(const mofft_core *c, const void *const *in_table,
                                          void *const *out_table, long long batch,

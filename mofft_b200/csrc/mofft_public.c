@@ -113,10 +113,25 @@ static mofft_status create_with_options(mofft_core **out, int precision_bits,
   }
   int chain[MOFFT_MAX_STAGES];
   int preferred[MOFFT_MAX_PASSES];
-  const int wisdom = mofft_wisdom_lookup(length, precision_bits, chain,
-                                         MOFFT_MAX_STAGES, preferred);
+  int wisdom = mofft_wisdom_lookup(length, precision_bits, chain,
+                                   MOFFT_MAX_STAGES, preferred);
   if (!wisdom && (options.flags & MOFFT_PLAN_STRICT_WISDOM))
     return MOFFT_WISDOM_NOT_FOUND;
+  /* A tuned schedule never costs memory the untuned one does not: three or
+   * more passes need a batch-sized workspace, which an out-of-place plan
+   * otherwise goes without, so such plans keep the model schedule (unless
+   * the caller insists on wisdom). */
+  if (wisdom && placement == MOFFT_OUT_OF_PLACE &&
+      !(options.flags & MOFFT_PLAN_STRICT_WISDOM)) {
+    int tuned_passes = 0;
+    while (tuned_passes < MOFFT_MAX_PASSES && preferred[tuned_passes] >= 0) ++tuned_passes;
+    mofft_plan_schedule model;
+    if (tuned_passes >= 3 &&
+        mofft_schedule_preview(precision_bits, length, NULL, 0, 0, &model, NULL, NULL) ==
+            MOFFT_SUCCESS &&
+        model.pass_count < 3)
+      wisdom = 0;
+  }
   status = mofft_core_create_tuned(out, precision_bits, length, batch, distance,
                                    direction, placement, wisdom ? chain : NULL,
                                    wisdom, preferred);

@@ -7,11 +7,16 @@
 // runs the group as ONE indirect batched launch on a free stream: host
 // payloads are staged into pooled device memory, a table of per-transform
 // device pointers is uploaded, the plan's passes run over the table, results
-// are copied back, and a host callback marks the group finished.  Up to
-// `streams` groups are in flight, so copies and kernels of different groups
-// overlap and new arrivals wait at most for one stream and enough memory.
+// are copied back, and an event recorded behind the work marks the group.
+// A lone request on device buffers skips the table and runs as a plain
+// batched launch.  Up to `streams` groups are in flight, so copies and
+// kernels of different groups overlap and new arrivals wait at most for one
+// stream and enough memory.  While groups are in flight the worker polls
+// their events every few microseconds (no host callback thread in the
+// completion path).
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -46,9 +51,9 @@ struct Block {
 
 struct Stream {
   cudaStream_t s = nullptr;
+  cudaEvent_t done = nullptr;  // recorded behind the group's work
   bool busy = false;
-  bool finished = false;
-  double t_done = 0.0;
+  bool recorded = false;       // `done` covers the current group
   std::vector<Req *> group;
   std::vector<Block> blocks;
   size_t admitted = 0;
@@ -56,8 +61,6 @@ struct Stream {
   void **d_table = nullptr;
   size_t table_cap = 0;       // entries per direction (in and out)
 };
-
-struct CallbackCtx;
 
 using PlanKey = std::tuple<size_t, int, int>;
 
@@ -73,7 +76,6 @@ struct mofft_server {
   std::unordered_map<uint64_t, Req *> reqs;
   uint64_t next_ticket = 1;
   std::vector<Stream> streams;
-  std::vector<CallbackCtx *> ctx;
   std::map<PlanKey, mofft_core *> plans;
   std::map<size_t, std::vector<void *>> pool;   // worker thread only
   size_t admitted = 0;
@@ -83,20 +85,6 @@ struct mofft_server {
 };
 
 namespace {
-
-struct CallbackCtx {
-  mofft_server *server;
-  int index;
-};
-
-void CUDART_CB group_finished(void *arg) {
-  CallbackCtx *c = static_cast<CallbackCtx *>(arg);
-  const double t = mofft_monotonic_seconds();
-  std::lock_guard<std::mutex> lock(c->server->mu);
-  c->server->streams[c->index].finished = true;
-  c->server->streams[c->index].t_done = t;
-  c->server->cv_work.notify_one();
-}
 
 size_t elem_bytes(int bits) { return bits == 32 ? 8 : 16; }
 
@@ -147,6 +135,17 @@ mofft_status launch_group(mofft_server *S, int idx) {
   const size_t eb = elem_bytes(head.precision_bits);
   const size_t n = head.length;
   const bool two_pass = plan->sched.pass_count > 1;
+  if (st.group.size() == 1) {
+    const Req *q = st.group.front();
+    const bool in_place = q->r.input == q->r.output;
+    if (!q->host_in && !q->host_out && !(in_place && two_pass) &&
+        plan->sched.pass_count <= 2) {
+      status = mofft_core_enqueue_batch(plan, q->r.input, q->r.output, q->r.batch, n, st.s);
+      if (status != MOFFT_SUCCESS) return status;
+      if (cudaEventRecord(st.done, st.s) != cudaSuccess) return MOFFT_INTERNAL_ERROR;
+      return MOFFT_SUCCESS;
+    }
+  }
   size_t transforms = 0;
   for (Req *q : st.group) transforms += q->r.batch;
   if (transforms > st.table_cap) {
@@ -221,8 +220,7 @@ mofft_status launch_group(mofft_server *S, int idx) {
   for (const Post &p : post)
     if (cudaMemcpyAsync(p.dst, p.src, p.bytes, p.kind, st.s) != cudaSuccess)
       return MOFFT_INTERNAL_ERROR;
-  if (cudaLaunchHostFunc(st.s, group_finished, S->ctx[idx]) != cudaSuccess)
-    return MOFFT_INTERNAL_ERROR;
+  if (cudaEventRecord(st.done, st.s) != cudaSuccess) return MOFFT_INTERNAL_ERROR;
   return MOFFT_SUCCESS;
 }
 
@@ -242,7 +240,7 @@ void finish_group(mofft_server *S, int idx, mofft_status status, double t_done) 
   S->admitted -= st.admitted;
   st.admitted = 0;
   st.busy = false;
-  st.finished = false;
+  st.recorded = false;
   S->cv_done.notify_all();
 }
 
@@ -298,7 +296,7 @@ bool form_group(mofft_server *S, int idx) {
     S->admitted += bytes;
     if (S->admitted > S->stats.peak_admitted_bytes) S->stats.peak_admitted_bytes = S->admitted;
     st.busy = true;
-    st.finished = false;
+    st.recorded = false;
     return true;
   }
   return false;
@@ -308,15 +306,24 @@ void worker_main(mofft_server *S) {
   cudaSetDevice(S->device);
   std::unique_lock<std::mutex> lock(S->mu);
   for (;;) {
-    for (size_t i = 0; i < S->streams.size(); ++i)
-      if (S->streams[i].busy && S->streams[i].finished)
-        finish_group(S, (int)i, MOFFT_SUCCESS, S->streams[i].t_done);
+    for (size_t i = 0; i < S->streams.size(); ++i) {
+      Stream &st = S->streams[i];
+      if (!st.busy || !st.recorded) continue;
+      const cudaError_t q = cudaEventQuery(st.done);
+      if (q == cudaSuccess) {
+        finish_group(S, (int)i, MOFFT_SUCCESS, mofft_monotonic_seconds());
+      } else if (q != cudaErrorNotReady) {
+        cudaGetLastError();
+        finish_group(S, (int)i, MOFFT_INTERNAL_ERROR, mofft_monotonic_seconds());
+      }
+    }
     int idx;
     while ((idx = free_stream(S)) >= 0 && form_group(S, idx)) {
       lock.unlock();
       const mofft_status st = launch_group(S, idx);
       lock.lock();
       ++S->stats.launches;
+      if (st == MOFFT_SUCCESS) S->streams[idx].recorded = true;
       if (st != MOFFT_SUCCESS) {
         // wait for whatever was already enqueued on the stream, then fail
         lock.unlock();
@@ -329,15 +336,17 @@ void worker_main(mofft_server *S) {
     bool busy = false;
     for (const Stream &s : S->streams) busy |= s.busy;
     if (S->stop && S->pending.empty() && !busy) break;
-    S->cv_work.wait(lock, [&] {
-      for (const Stream &s : S->streams)
-        if (s.busy && s.finished) return true;
+    auto startable = [&] {
       if (S->stop) return true;
       if (S->pending.empty()) return false;
       if (free_stream(S) < 0) return false;
       return S->admitted + S->pending.front()->payload <= S->opt.hbm_budget_bytes ||
              S->admitted == 0;
-    });
+    };
+    if (busy)   // poll the in-flight groups' events
+      S->cv_work.wait_for(lock, std::chrono::microseconds(10), startable);
+    else
+      S->cv_work.wait(lock, startable);
   }
 }
 
@@ -367,12 +376,12 @@ extern "C" mofft_status mofft_server_create(mofft_server **out,
   cudaGetDevice(&S->device);
   S->streams.resize((size_t)S->opt.streams);
   for (int i = 0; i < S->opt.streams; ++i) {
-    if (cudaStreamCreateWithFlags(&S->streams[i].s, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&S->streams[i].s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&S->streams[i].done, cudaEventDisableTiming) != cudaSuccess) {
       cudaGetLastError();
       mofft_server_destroy(S);
       return MOFFT_INTERNAL_ERROR;
     }
-    S->ctx.push_back(new CallbackCtx{S, i});
   }
   S->worker = std::thread(worker_main, S);
   *out = S;
@@ -446,12 +455,12 @@ extern "C" void mofft_server_destroy(mofft_server *S) {
     if (st.s) cudaStreamSynchronize(st.s);
     if (st.h_table) cudaFreeHost(st.h_table);
     if (st.d_table) cudaFree(st.d_table);
+    if (st.done) cudaEventDestroy(st.done);
     if (st.s) cudaStreamDestroy(st.s);
   }
   for (auto &kv : S->pool)
     for (void *p : kv.second) cudaFree(p);
   for (auto &kv : S->plans) mofft_core_destroy(kv.second);
   for (auto &kv : S->reqs) delete kv.second;
-  for (CallbackCtx *c : S->ctx) delete c;
   delete S;
 }

@@ -298,3 +298,17 @@ def test_bound_array_measure_equals_pretuned_result():
     assert oracle.rel_l2(y1, ref) <= 5e-7 * 12 and oracle.rel_l2(y2, ref) <= 5e-7 * 12
     fn("plan_destroy", 32)(p1)
     fn("plan_destroy", 32)(p2)
+
+
+def test_tuned_three_pass_only_where_a_workspace_exists_anyway():
+    """FP64 n = 2^20: the compiled wisdom holds a three-pass schedule.  In
+    place (which needs a batch-sized workspace in any case) the plan uses it;
+    out of place the plan keeps the two-pass model schedule, which needs no
+    workspace, so tuning never costs memory."""
+    n = 1 << 20
+    with m.Plan.create(n, m.FORWARD, m.IN_PLACE, bits=64, batch=2) as p:
+        s = p.schedule()
+        assert s["pass_count"] == 3 and s["workspace_bytes"] > 0
+    with m.Plan.create(n, m.FORWARD, m.OUT_OF_PLACE, bits=64, batch=2) as p:
+        s = p.schedule()
+        assert s["pass_count"] == 2 and s["workspace_bytes"] == 0
