@@ -124,7 +124,7 @@ struct RowsLayout {
   }
 };
 
-template <typename T, int C, int PITCH>
+template <typename T, int C, int PITCH, bool TW>
 struct ColsLayout {
   T* sre;          // shared base of the tile (all C lines)
   T* sim;
@@ -138,15 +138,18 @@ struct ColsLayout {
   // super-stage twiddle on load: W^{e}, e = jmod * i, two-level table
   const cplx_t<T>* tw_hi;
   const cplx_t<T>* tw_lo;
-  long long jmod;         // (j mod Ns_outer) of this line, 0 = no twiddle
+  long long jmod;         // (j mod Ns_outer) of this line
   int split_shift;        // K = 1 << split_shift
   __device__ __forceinline__ int saddr(int i) const { return i * PITCH + c; }
+  // TW (passes with Ns_outer > 1): every element is multiplied by
+  // W^{jmod i}, without a branch (entry 0 of both tables is exactly 1, so
+  // e = 0 leaves the value unchanged) so that all loads can issue together.
   __device__ __forceinline__ void gload(int i, T& re, T& im) const {
     if (active) {
       const cplx_t<T> v = ld_global<T>(gin + (long long)i * in_stride);
       re = v.x;
       im = v.y * sign_in;
-      if (jmod != 0 && i != 0) {
+      if constexpr (TW) {
         const long long e = jmod * (long long)i;
         const cplx_t<T> hi = __ldg(tw_hi + (e >> split_shift));
         const cplx_t<T> lo = __ldg(tw_lo + (e & ((1LL << split_shift) - 1)));
@@ -576,23 +579,18 @@ struct ColsGeom {
   static constexpr int THREADS = TPL * C;
 };
 
-// Body of one COLS tile: lines j0 .. j0+C-1 of batch entry b, run by threads
-// 0 .. TPL*C-1 of the CTA (every thread of the CTA must call it).
-template <typename T, int L, int TPL, int C, int... Rs>
-__device__ __forceinline__ void cols_body(const ColsArgs<T>& a, long long b,
-                                          long long j0, unsigned char* smem_raw) {
-  static_assert(StageProduct<L, Rs...>::value == L, "radices must multiply to L");
+// Addressing of this thread's line of a COLS tile (lines j0 .. j0+C-1 of
+// batch entry b).
+template <typename T, int L, int TPL, int C, bool TW, class Layout>
+__device__ __forceinline__ void cols_layout(Layout& lay, const ColsArgs<T>& a, long long b,
+                                            long long j0, T* sre, T* sim) {
   using G = ColsGeom<T, L, TPL, C>;
-  T* sre = reinterpret_cast<T*>(smem_raw);
-  T* sim = sre + G::WORDS;
   const long long lines_total = a.total / L;            // M / L
   const int c = threadIdx.x % C;
-  const int t = threadIdx.x / C;
   const long long j = j0 + c;
   const long long ns = a.ns_outer;
   const long long jq = j / ns;
   const long long jm = j - jq * ns;
-  ColsLayout<T, C, G::PITCH> lay;
   lay.sre = sre;
   lay.sim = sim;
   lay.c = c;
@@ -609,10 +607,25 @@ __device__ __forceinline__ void cols_body(const ColsArgs<T>& a, long long b,
   lay.tw_lo = a.tw_lo;
   lay.jmod = jm;
   lay.split_shift = a.split_shift;
-  if (ns == 1) {
+  (void)G::THREADS;
+}
+
+// Body of one COLS tile: lines j0 .. j0+C-1 of batch entry b, run by threads
+// 0 .. TPL*C-1 of the CTA (every thread of the CTA must call it).
+template <typename T, int L, int TPL, int C, int... Rs>
+__device__ __forceinline__ void cols_body(const ColsArgs<T>& a, long long b,
+                                          long long j0, unsigned char* smem_raw) {
+  static_assert(StageProduct<L, Rs...>::value == L, "radices must multiply to L");
+  using G = ColsGeom<T, L, TPL, C>;
+  T* sre = reinterpret_cast<T*>(smem_raw);
+  T* sim = sre + G::WORDS;
+  const int t = threadIdx.x / C;
+  if (a.ns_outer == 1) {
+    ColsLayout<T, C, G::PITCH, false> lay;
+    cols_layout<T, L, TPL, C, false>(lay, a, b, j0, sre, sim);
     StageRunner<T, L, TPL, 1, 0, false, true, true, false, Rs...>::run(lay, t, a.tw);
     // lines j0..j0+C-1 are contiguous: out[b*dist + j0*L + c*L + k]
-    cplx_t<T>* dst = out_b + j0 * L;
+    cplx_t<T>* dst = batch_out<T>(a.out, a.out_dist, a.out_table, b) + j0 * L;
     if (lay.active) {
       for (int q = threadIdx.x; q < C * L; q += G::THREADS) {
         const int cc = q / L;
@@ -622,6 +635,8 @@ __device__ __forceinline__ void cols_body(const ColsArgs<T>& a, long long b,
       }
     }
   } else {
+    ColsLayout<T, C, G::PITCH, true> lay;
+    cols_layout<T, L, TPL, C, true>(lay, a, b, j0, sre, sim);
     StageRunner<T, L, TPL, 1, 0, false, false, true, false, Rs...>::run(lay, t, a.tw);
   }
 }
