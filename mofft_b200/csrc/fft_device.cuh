@@ -122,6 +122,8 @@ struct RowsLayout {
   __device__ __forceinline__ void gstore(int i, T re, T im) const {
     if (active) st_global<T>(gout + i, re, im * sign);
   }
+  template <int R>
+  __device__ __forceinline__ void super_twiddle(int, int, T (&)[R], T (&)[R]) const {}
 };
 
 template <typename T, int C, int PITCH, bool TW>
@@ -141,25 +143,63 @@ struct ColsLayout {
   long long jmod;         // (j mod Ns_outer) of this line
   int split_shift;        // K = 1 << split_shift
   __device__ __forceinline__ int saddr(int i) const { return i * PITCH + c; }
-  // TW (passes with Ns_outer > 1): every element is multiplied by
-  // W^{jmod i}, without a branch (entry 0 of both tables is exactly 1, so
-  // e = 0 leaves the value unchanged) so that all loads can issue together.
   __device__ __forceinline__ void gload(int i, T& re, T& im) const {
     if (active) {
       const cplx_t<T> v = ld_global<T>(gin + (long long)i * in_stride);
       re = v.x;
       im = v.y * sign_in;
-      if constexpr (TW) {
-        const long long e = jmod * (long long)i;
-        const cplx_t<T> hi = __ldg(tw_hi + (e >> split_shift));
-        const cplx_t<T> lo = __ldg(tw_lo + (e & ((1LL << split_shift) - 1)));
-        T wr = hi.x, wi = hi.y;
-        cmul<T>(wr, wi, lo.x, lo.y);
-        cmul<T>(re, im, wr, wi);
-      }
     } else {
       re = T(0);
       im = T(0);
+    }
+  }
+  // W^e from the two-level table (entry 0 of both tables is exactly 1).
+  __device__ __forceinline__ void super_w(long long e, T& wr, T& wi) const {
+    const cplx_t<T> hi = __ldg(tw_hi + (e >> split_shift));
+    const cplx_t<T> lo = __ldg(tw_lo + (e & ((1LL << split_shift) - 1)));
+    wr = hi.x;
+    wi = hi.y;
+    cmul<T>(wr, wi, lo.x, lo.y);
+  }
+  // Super-stage twiddle of butterfly j's loaded inputs (TW: passes with
+  // Ns_outer > 1): v[r] *= W^{jmod (j + r BF)}, no branch, so that every
+  // load issues together.  For R = 16 it is W^{jmod j} (W^{jmod BF})^r with
+  // the powers formed from w, w^2, w^4, w^8 as in twiddle16_derived: five
+  // table lookups instead of sixteen.
+  template <int R>
+  __device__ __forceinline__ void super_twiddle(int j, int BF, T (&vr)[R], T (&vi)[R]) const {
+    if constexpr (TW) {
+      if constexpr (R == 16) {
+        T wr[16], wi[16];
+        T br, bi;
+        super_w(jmod * (long long)j, br, bi);
+        const long long u = jmod * (long long)BF;
+        super_w(u, wr[1], wi[1]);
+        super_w(2 * u, wr[2], wi[2]);
+        super_w(4 * u, wr[4], wi[4]);
+        super_w(8 * u, wr[8], wi[8]);
+#define MOFFT_UMUL(D, A, B)                          \
+  wr[D] = wr[A] * wr[B] - wi[A] * wi[B];             \
+  wi[D] = wr[A] * wi[B] + wi[A] * wr[B];
+        MOFFT_UMUL(3, 2, 1) MOFFT_UMUL(5, 4, 1) MOFFT_UMUL(6, 4, 2) MOFFT_UMUL(7, 4, 3)
+        MOFFT_UMUL(9, 8, 1) MOFFT_UMUL(10, 8, 2) MOFFT_UMUL(11, 8, 3) MOFFT_UMUL(12, 8, 4)
+        MOFFT_UMUL(13, 8, 5) MOFFT_UMUL(14, 8, 6) MOFFT_UMUL(15, 8, 7)
+#undef MOFFT_UMUL
+        cmul<T>(vr[0], vi[0], br, bi);
+#pragma unroll
+        for (int r = 1; r < 16; ++r) {
+          T xr = wr[r], xi = wi[r];
+          cmul<T>(xr, xi, br, bi);
+          cmul<T>(vr[r], vi[r], xr, xi);
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          T xr, xi;
+          super_w(jmod * (long long)(j + r * BF), xr, xi);
+          cmul<T>(vr[r], vi[r], xr, xi);
+        }
+      }
     }
   }
   __device__ __forceinline__ void gstore(int i, T re, T im) const {
@@ -221,6 +261,7 @@ __device__ __forceinline__ void reg_stage(const Layout& lay, int t,
           vi[m][r] = lay.sim[lay.saddr(idx)];
         }
       }
+      if constexpr (SRC == kGlobal) lay.template super_twiddle<R>(j, BF, vr[m], vi[m]);
       if (NS > 1) {
         const int jm = j % NS;
         if constexpr (DTW && R == 16) {
