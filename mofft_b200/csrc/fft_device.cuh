@@ -163,32 +163,33 @@ struct ColsLayout {
   }
   // Super-stage twiddle of butterfly j's loaded inputs (TW: passes with
   // Ns_outer > 1): v[r] *= W^{jmod (j + r BF)}, no branch, so that every
-  // load issues together.  For R = 16 it is W^{jmod j} (W^{jmod BF})^r with
-  // the powers formed from w, w^2, w^4, w^8 as in twiddle16_derived: five
-  // table lookups instead of sixteen.
+  // load issues together.  For R <= 16 it is W^{jmod j} u^r with
+  // u = W^{jmod BF}: u, u^2, u^4, u^8 come from the table and every other
+  // power is a product of two earlier ones (at most three products in a
+  // chain), so a butterfly needs at most five lookups instead of R.
   template <int R>
   __device__ __forceinline__ void super_twiddle(int j, int BF, T (&vr)[R], T (&vi)[R]) const {
     if constexpr (TW) {
-      if constexpr (R == 16) {
-        T wr[16], wi[16];
+      if constexpr (R <= 16) {
+        T ur[R], ui[R];
         T br, bi;
         super_w(jmod * (long long)j, br, bi);
         const long long u = jmod * (long long)BF;
-        super_w(u, wr[1], wi[1]);
-        super_w(2 * u, wr[2], wi[2]);
-        super_w(4 * u, wr[4], wi[4]);
-        super_w(8 * u, wr[8], wi[8]);
-#define MOFFT_UMUL(D, A, B)                          \
-  wr[D] = wr[A] * wr[B] - wi[A] * wi[B];             \
-  wi[D] = wr[A] * wi[B] + wi[A] * wr[B];
-        MOFFT_UMUL(3, 2, 1) MOFFT_UMUL(5, 4, 1) MOFFT_UMUL(6, 4, 2) MOFFT_UMUL(7, 4, 3)
-        MOFFT_UMUL(9, 8, 1) MOFFT_UMUL(10, 8, 2) MOFFT_UMUL(11, 8, 3) MOFFT_UMUL(12, 8, 4)
-        MOFFT_UMUL(13, 8, 5) MOFFT_UMUL(14, 8, 6) MOFFT_UMUL(15, 8, 7)
-#undef MOFFT_UMUL
+#pragma unroll
+        for (int k = 1; k < R; k <<= 1) super_w(u * k, ur[k], ui[k]);
+#pragma unroll
+        for (int r = 3; r < R; ++r) {
+          if ((r & (r - 1)) == 0) continue;          // a power of two: loaded
+          int h = 1;
+          while (h * 2 <= r) h *= 2;                 // highest power of two in r
+          const int l = r - h;
+          ur[r] = ur[h] * ur[l] - ui[h] * ui[l];
+          ui[r] = ur[h] * ui[l] + ui[h] * ur[l];
+        }
         cmul<T>(vr[0], vi[0], br, bi);
 #pragma unroll
-        for (int r = 1; r < 16; ++r) {
-          T xr = wr[r], xi = wi[r];
+        for (int r = 1; r < R; ++r) {
+          T xr = ur[r], xi = ui[r];
           cmul<T>(xr, xi, br, bi);
           cmul<T>(vr[r], vi[r], xr, xi);
         }

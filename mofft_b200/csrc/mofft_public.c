@@ -117,19 +117,20 @@ static mofft_status create_with_options(mofft_core **out, int precision_bits,
                                    MOFFT_MAX_STAGES, preferred);
   if (!wisdom && (options.flags & MOFFT_PLAN_STRICT_WISDOM))
     return MOFFT_WISDOM_NOT_FOUND;
-  /* A tuned schedule never costs memory the untuned one does not: three or
-   * more passes need a batch-sized workspace, which an out-of-place plan
-   * otherwise goes without, so such plans keep the model schedule (unless
-   * the caller insists on wisdom). */
-  if (wisdom && placement == MOFFT_OUT_OF_PLACE &&
-      !(options.flags & MOFFT_PLAN_STRICT_WISDOM)) {
+  /* A tuned schedule never costs memory the untuned one does not: a
+   * schedule of three or more passes, or of two passes in place, needs a
+   * batch-sized workspace; when the tuned schedule needs one and the model
+   * schedule does not, the plan keeps the model schedule (unless the caller
+   * insists on wisdom). */
+  if (wisdom && !(options.flags & MOFFT_PLAN_STRICT_WISDOM)) {
     int tuned_passes = 0;
     while (tuned_passes < MOFFT_MAX_PASSES && preferred[tuned_passes] >= 0) ++tuned_passes;
+    const int in_place = placement == MOFFT_IN_PLACE;
     mofft_plan_schedule model;
-    if (tuned_passes >= 3 &&
+    if ((tuned_passes >= 3 || (tuned_passes == 2 && in_place)) &&
         mofft_schedule_preview(precision_bits, length, NULL, 0, 0, &model, NULL, NULL) ==
             MOFFT_SUCCESS &&
-        model.pass_count < 3)
+        !(model.pass_count >= 3 || (model.pass_count == 2 && in_place)))
       wisdom = 0;
   }
   status = mofft_core_create_tuned(out, precision_bits, length, batch, distance,
