@@ -229,7 +229,9 @@ def cpu_baseline(n: int, bits: int, direction: int, seconds: float) -> dict:
     dtype = np.complex64 if bits == 32 else np.complex128
     batch = max(cores, (1 << 22) // n)
     x = oracle.uniform(n * batch, seed=n, dtype=dtype).reshape(batch, n)
-    oracle.fft_port(x[:cores], direction, threads=cores)          # warm-up
+    t_warm = time.perf_counter() + 0.25                          # warm-up >= 0.25 s
+    while time.perf_counter() < t_warm:
+        oracle.fft_port(x[:cores], direction, threads=cores)
     samples = []
     t_end = time.perf_counter() + seconds
     while time.perf_counter() < t_end or len(samples) < 3:
@@ -240,7 +242,8 @@ def cpu_baseline(n: int, bits: int, direction: int, seconds: float) -> dict:
             break
     med = statistics.median(samples)
     value = flops_per_transform(n) * batch / med / 1e9
-    extra = {}
+    cv = statistics.pstdev(samples) / statistics.mean(samples) if len(samples) > 1 else 0.0
+    extra = {"cv": round(cv, 4)}
     try:
         import scipy.fft
         t0 = time.perf_counter()
@@ -279,6 +282,7 @@ def run_reference(args, world, rank):
         times.append(time.perf_counter() - t0)
     ms = 1e3 * sum(times) / len(times)
     value = flops_per_transform(n) * batch / (ms / 1e3) / 1e9
+    cv = statistics.pstdev(times) / statistics.mean(times) if len(times) > 1 else 0.0
     line = {
         "impl": "reference", "metric": "C2C GFLOP/s (5n log2 n)", "value": round(value, 3),
         "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -286,7 +290,7 @@ def run_reference(args, world, rank):
         "vs_baseline": None, "dtype": "f32" if bits == 32 else "f64", "data": "synthetic",
         "config": workload_config(args),
         "cpu_baseline": {"value": round(value, 3), "unit": "GFLOP/s", "cores": cores,
-                         "kind": "port",
+                         "kind": "port", "cv": round(cv, 4),
                          "sample": f"{batch} transforms of n={n} per step (the reference's "
                                    "SME kernels cannot run on x86; FFTW 3.3.11: unavailable "
                                    "on this box)"},
