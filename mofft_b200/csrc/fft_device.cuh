@@ -50,6 +50,21 @@ __host__ __device__ constexpr int spad(int a) { return a + (a >> Pad<T>::shift);
 template <typename T>
 __host__ __device__ constexpr int spad_len(int n) { return n + (n >> Pad<T>::shift) + 1; }
 
+// Shared-memory words between the lines of a multi-line ROWS tile: at least
+// spad_len(L), rounded up so that the line pitch is congruent to the threads
+// per line modulo one 128-byte bank row.  The threads of a warp then spread
+// the lines they work on over disjoint banks (a bank simulation of the
+// staged kernels' copies and exchanges: 1.5-1.7 -> 1.2-1.5 wavefronts per
+// access for most instances).  One-line tiles keep spad_len(L).
+template <typename T>
+__host__ __device__ constexpr int rows_line(int L, int TPL, int TB) {
+  const int row = sizeof(T) == 4 ? 32 : 16;
+  int b = spad_len<T>(L);
+  if (TB > 1)
+    while (b % row != TPL % row) ++b;
+  return b;
+}
+
 template <typename T>
 __device__ __forceinline__ void cmul(T& xr, T& xi, T wr, T wi) {
   const T r = xr * wr - xi * wi;
@@ -477,7 +492,7 @@ __device__ __forceinline__ void rows_body(const RowsArgs<T>& a, long long b0,
   static_assert(StageProduct<L, Rs...>::value == L, "radices must multiply to L");
   constexpr bool STAGED = (FLAGS & kStaged) != 0;
   constexpr bool DTW = (FLAGS & kDerivedTw) != 0;
-  constexpr int LINE = spad_len<T>(L);
+  constexpr int LINE = rows_line<T>(L, TPL, TB);
   T* sre = reinterpret_cast<T*>(smem_raw);
   T* sim = sre + TB * LINE;
   const int line = threadIdx.x / TPL;

@@ -55,7 +55,7 @@ ColsArgs<T> cols_args(const mofft_pass_args *p) {
 template <typename T, int L, int TPL, int TB, int FLAGS, int... Rs>
 struct RowsInst {
   static constexpr size_t smem() {
-    return ((FLAGS & kSplitX) ? 1ull : 2ull) * TB * spad_len<T>(L) * sizeof(T);
+    return ((FLAGS & kSplitX) ? 1ull : 2ull) * TB * rows_line<T>(L, TPL, TB) * sizeof(T);
   }
   static const void *func() {
     return reinterpret_cast<const void *>(&rows_kernel<T, L, TPL, TB, FLAGS, Rs...>);

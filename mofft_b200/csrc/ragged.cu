@@ -101,7 +101,7 @@ constexpr int kArgCount = (int)sizeof...(R);
 
 #define MOFFT_ROWS_INFO(ID, L, TPL, ST, ...)                         \
   {ID, L, TPL, 0, kArgCount<__VA_ARGS__>, {__VA_ARGS__},             \
-   2ull * (kThreads / TPL) * spad_len<float>(L) * sizeof(float)},
+   2ull * (kThreads / TPL) * rows_line<float>(L, TPL, kThreads / TPL) * sizeof(float)},
 #define MOFFT_COLS_INFO(ID, L, TPL, ...)                             \
   {ID, L, TPL, 1, kArgCount<__VA_ARGS__>, {__VA_ARGS__},             \
    ColsGeom<float, L, TPL, kColsLines>::SMEM},
