@@ -561,7 +561,8 @@ def run_serve(args, world, rank, local):
     batching, 4 streams, 40 GiB admission) and serial plain execution (one
     blocking plan execute per request, plans created beforehand) process the
     same requests: all at t=0 (saturation) and at Poisson rates of 50 % and
-    90 % of the serial capacity."""
+    90 % of the serial capacity.  At saturation the one-shot pattern (plan,
+    execute, destroy per request) is timed as well."""
     import threading
 
     import numpy as np
@@ -607,6 +608,24 @@ def run_serve(args, world, rank, local):
             assert st == 0
             offset += nbytes
             lat.append(time.perf_counter() - t0 - a)
+        return time.perf_counter() - t0, lat
+
+    def run_serial_one_shot():
+        # the reference API's one-shot pattern: plan, execute, destroy per request
+        lat = []
+        t0 = time.perf_counter()
+        offset = 0
+        for r in reqs:
+            nbytes = r["n"] * r["batch"] * (8 if r["bits"] == 32 else 16)
+            if offset + nbytes > ring_bytes:
+                offset = 0
+            p = m.Plan.create(r["n"], r["direction"], m.OUT_OF_PLACE, bits=r["bits"],
+                              batch=r["batch"])
+            st = p.execute_ptr(arena_in[r["bits"]].data_ptr(), out_ptr(offset))
+            p.destroy()
+            assert st == 0
+            offset += nbytes
+            lat.append(time.perf_counter() - t0)
         return time.perf_counter() - t0, lat
 
     def run_server(arrivals):
@@ -655,6 +674,7 @@ def run_serve(args, world, rank, local):
 
     zeros = [0.0] * len(reqs)
     serial_span, serial_lat = run_serial(zeros)
+    one_shot_span, one_shot_lat = run_serial_one_shot()
     srv_span, srv_lat, stats = run_server(zeros)
     capacity = len(reqs) / serial_span           # serial requests per second
     rates = {}
@@ -681,6 +701,8 @@ def run_serve(args, world, rank, local):
                    "server": {"streams": 4, "hbm_budget_gib": 40}},
         "saturation": {"server": sat_server, "serial_plain": sat_serial,
                        "speedup": round(serial_span / srv_span, 2),
+                       "serial_plan_per_request": summary(one_shot_span, one_shot_lat),
+                       "speedup_vs_plan_per_request": round(one_shot_span / srv_span, 2),
                        "launches": stats["launches"], "requests": len(reqs)},
         "poisson": rates,
     }

@@ -227,6 +227,7 @@ struct ColsLayout {
 constexpr int kStaged = 1;       // I/O staged through shared memory
 constexpr int kDerivedTw = 2;    // radix-16 twiddles from w, w^2, w^4, w^8
 constexpr int kSplitX = 4;       // exchanges move one component at a time
+constexpr int kTwoCtas = 8;      // registers capped for two resident CTAs per SM
 
 // Twiddles of one radix-16 butterfly: v[r] *= w^r.  Loads the table entries
 // of w^1, w^2, w^4 and w^8 and forms the other powers with at most three
@@ -595,7 +596,7 @@ __device__ __forceinline__ void rows_body(const RowsArgs<T>& a, long long b0,
 }
 
 template <typename T, int L, int TPL, int TB, int FLAGS, int... Rs>
-__global__ void __launch_bounds__(TPL * TB)
+__global__ void __launch_bounds__(TPL * TB, (FLAGS & kTwoCtas) ? 2 : 1)
 rows_kernel(const RowsArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   rows_body<T, L, TPL, TB, FLAGS, Rs...>(a, (long long)blockIdx.x * TB, smem_raw);

@@ -212,6 +212,9 @@ struct GenericInst {
 #define ROWSX(T, L, TPL, TB, ...) \
   RowsInst<T, L, TPL, TB, kDerivedTw | kSplitX, __VA_ARGS__>::entry( \
       "rows_" #T "_" #L "_t" #TPL "_b" #TB "_sfalse_dx")
+#define ROWSD2(T, L, TPL, TB, ...) \
+  RowsInst<T, L, TPL, TB, kDerivedTw | kTwoCtas, __VA_ARGS__>::entry( \
+      "rows_" #T "_" #L "_t" #TPL "_b" #TB "_sfalse_d2")
 #define COLS(T, L, TPL, C, ...) \
   ColsInst<T, L, TPL, C, __VA_ARGS__>::entry("cols_" #T "_" #L "_t" #TPL "_c" #C)
 

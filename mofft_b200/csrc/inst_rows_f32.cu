@@ -33,6 +33,11 @@ const Entry *entries_rows_f32(int *count) {
       ROWSD(float, 4096, 512, 1, false, 16, 16, 16),
       ROWSD(float, 8192, 512, 1, false, 16, 16, 16, 2),
       ROWSD(float, 16384, 512, 1, false, 16, 16, 16, 4),
+      // radix-32 stages: one exchange fewer for the long lines
+      ROWSD2(float, 8192, 256, 1, 32, 16, 16),
+      ROWSD2(float, 8192, 256, 1, 16, 16, 32),
+      ROWSD(float, 16384, 512, 1, false, 32, 32, 16),
+      ROWSD(float, 16384, 512, 1, false, 16, 32, 32),
       // split exchanges (one component at a time: half the shared memory)
       ROWSX(float, 2048, 128, 2, 16, 16, 8),
       ROWSX(float, 4096, 256, 1, 16, 16, 16),
