@@ -596,8 +596,16 @@ __device__ __forceinline__ void rows_body(const RowsArgs<T>& a, long long b0,
 }
 
 template <typename T, int L, int TPL, int TB, int FLAGS, int... Rs>
-__global__ void __launch_bounds__(TPL * TB, (FLAGS & kTwoCtas) ? 2 : 1)
+__global__ void __launch_bounds__(TPL * TB)
 rows_kernel(const RowsArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  rows_body<T, L, TPL, TB, FLAGS, Rs...>(a, (long long)blockIdx.x * TB, smem_raw);
+}
+
+// The same with registers capped for two resident CTAs per SM (kTwoCtas).
+template <typename T, int L, int TPL, int TB, int FLAGS, int... Rs>
+__global__ void __launch_bounds__(TPL * TB, 2)
+rows_kernel_2cta(const RowsArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   rows_body<T, L, TPL, TB, FLAGS, Rs...>(a, (long long)blockIdx.x * TB, smem_raw);
 }

@@ -58,15 +58,22 @@ struct RowsInst {
     return ((FLAGS & kSplitX) ? 1ull : 2ull) * TB * rows_line<T>(L, TPL, TB) * sizeof(T);
   }
   static const void *func() {
-    return reinterpret_cast<const void *>(&rows_kernel<T, L, TPL, TB, FLAGS, Rs...>);
+    if constexpr ((FLAGS & kTwoCtas) != 0)
+      return reinterpret_cast<const void *>(&rows_kernel_2cta<T, L, TPL, TB, FLAGS, Rs...>);
+    else
+      return reinterpret_cast<const void *>(&rows_kernel<T, L, TPL, TB, FLAGS, Rs...>);
   }
   static cudaError_t launch(const mofft_pass_args *p, cudaStream_t s) {
     if (p->conj_in != p->conj_out) return cudaErrorInvalidValue;
     const long long grid = (p->batch + TB - 1) / TB;
     if (grid <= 0) return cudaSuccess;
     if (grid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-    rows_kernel<T, L, TPL, TB, FLAGS, Rs...>
-        <<<(unsigned)grid, TPL * TB, smem(), s>>>(rows_args<T>(p));
+    if constexpr ((FLAGS & kTwoCtas) != 0)
+      rows_kernel_2cta<T, L, TPL, TB, FLAGS, Rs...>
+          <<<(unsigned)grid, TPL * TB, smem(), s>>>(rows_args<T>(p));
+    else
+      rows_kernel<T, L, TPL, TB, FLAGS, Rs...>
+          <<<(unsigned)grid, TPL * TB, smem(), s>>>(rows_args<T>(p));
     return cudaGetLastError();
   }
   static Entry entry(const char *name) {

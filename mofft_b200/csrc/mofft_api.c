@@ -588,6 +588,7 @@ void mofft_core_destroy(mofft_core *c) {
   if (saved != c->device) cudaSetDevice(c->device);
   release_device(c);
   if (c->stream) cudaStreamDestroy((cudaStream_t)c->stream);
+  if (c->stream2) cudaStreamDestroy((cudaStream_t)c->stream2);
   if (saved >= 0 && saved != c->device) cudaSetDevice(saved);
   pthread_mutex_destroy(&c->lock);
   free(c);
@@ -854,6 +855,10 @@ static int is_device_pointer(const void *p) {
   return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
 }
 
+static mofft_status enqueue_with_work(const mofft_core *c, const void *in, void *out,
+                                      size_t batch, size_t distance, void *work,
+                                      void *stream);
+
 /* Enqueue the plan's passes: in -> out on `stream` (device pointers). */
 mofft_status mofft_core_enqueue(const mofft_core *c, const void *in, void *out,
                                 void *stream) {
@@ -865,6 +870,15 @@ mofft_status mofft_core_enqueue(const mofft_core *c, const void *in, void *out,
  * the plan's workspace needs batch <= the plan's batch. */
 mofft_status mofft_core_enqueue_batch(const mofft_core *c, const void *in, void *out,
                                       size_t batch, size_t distance, void *stream) {
+  if (c->d_work && batch > c->batch) return MOFFT_INTERNAL_ERROR;
+  return enqueue_with_work(c, in, out, batch, distance, c->d_work, stream);
+}
+
+/* Passes of c over `batch` transforms; `work` (dense, batch x length
+ * elements, or NULL) is the intermediate buffer of schedules that need one. */
+static mofft_status enqueue_with_work(const mofft_core *c, const void *in, void *out,
+                                      size_t batch, size_t distance, void *work,
+                                      void *stream) {
   const size_t cb = mofft_complex_bytes(c->precision_bits);
   const int P = c->sched.pass_count;
   const int backward = c->direction == MOFFT_BACKWARD;
@@ -882,8 +896,8 @@ mofft_status mofft_core_enqueue_batch(const mofft_core *c, const void *in, void 
       dst = out;
       dst_dist = (long long)distance;
     } else {
-      if (!c->d_work || batch > c->batch) return MOFFT_INTERNAL_ERROR;
-      dst = c->d_work;
+      if (!work) return MOFFT_INTERNAL_ERROR;
+      dst = work;
       dst_dist = (long long)c->length;
     }
     mofft_pass_args a;
@@ -925,6 +939,14 @@ mofft_status mofft_core_enqueue_batch(const mofft_core *c, const void *in, void 
 
 static mofft_status ensure_staging(mofft_core *c) {
   const size_t bytes = c->batch * c->distance * mofft_complex_bytes(c->precision_bits);
+  if (!c->stream2) {
+    cudaStream_t s2;
+    if (cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      return MOFFT_INTERNAL_ERROR;
+    }
+    c->stream2 = s2;
+  }
   if (c->stage_bytes >= bytes && c->d_stage[0] && c->d_stage[1])
     return MOFFT_SUCCESS;
   if (c->d_stage[0]) cudaFree(c->d_stage[0]);
@@ -973,21 +995,39 @@ mofft_status mofft_core_execute(const mofft_core *cc, const void *in, void *out)
     pthread_mutex_lock(&c->lock);
     st = ensure_staging(c);
     if (st == MOFFT_SUCCESS) {
+      /* Chunks of about 64 MiB alternate between two streams, so the upload
+       * of one chunk, the passes of another and the download of a third
+       * overlap (copies from and to pinned memory run on separate engines). */
       const size_t cb = mofft_complex_bytes(c->precision_bits);
       const size_t span = ((c->batch - 1) * c->distance + c->length) * cb;
-      stream = c->stream;
-      if (cudaMemcpyAsync(c->d_stage[0], in, span, cudaMemcpyHostToDevice,
-                          (cudaStream_t)stream) != cudaSuccess)
-        st = MOFFT_INTERNAL_ERROR;
-      if (st == MOFFT_SUCCESS)
-        st = mofft_core_enqueue(c, c->d_stage[0], c->d_stage[1], stream);
-      if (st == MOFFT_SUCCESS &&
-          cudaMemcpyAsync(out, c->d_stage[1], span, cudaMemcpyDeviceToHost,
-                          (cudaStream_t)stream) != cudaSuccess)
-        st = MOFFT_INTERNAL_ERROR;
-      if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess &&
-          st == MOFFT_SUCCESS)
-        st = MOFFT_INTERNAL_ERROR;
+      const size_t chunk_bytes = (size_t)64 << 20;
+      size_t chunks = (span + chunk_bytes - 1) / chunk_bytes;
+      if (chunks > c->batch) chunks = c->batch;
+      if (chunks > 64) chunks = 64;
+      if (chunks < 1) chunks = 1;
+      cudaStream_t streams[2] = {(cudaStream_t)c->stream, (cudaStream_t)c->stream2};
+      for (size_t k = 0; k < chunks && st == MOFFT_SUCCESS; ++k) {
+        const size_t b0 = k * c->batch / chunks, b1 = (k + 1) * c->batch / chunks;
+        if (b1 == b0) continue;
+        const size_t off = b0 * c->distance * cb;
+        const size_t bytes = ((b1 - b0 - 1) * c->distance + c->length) * cb;
+        cudaStream_t s = streams[k & 1];
+        unsigned char *din = (unsigned char *)c->d_stage[0] + off;
+        unsigned char *dout = (unsigned char *)c->d_stage[1] + off;
+        void *work = c->d_work ? (unsigned char *)c->d_work + b0 * c->length * cb : NULL;
+        if (cudaMemcpyAsync(din, (const unsigned char *)in + off, bytes,
+                            cudaMemcpyHostToDevice, s) != cudaSuccess)
+          st = MOFFT_INTERNAL_ERROR;
+        if (st == MOFFT_SUCCESS)
+          st = enqueue_with_work(c, din, dout, b1 - b0, c->distance, work, s);
+        if (st == MOFFT_SUCCESS &&
+            cudaMemcpyAsync((unsigned char *)out + off, dout, bytes, cudaMemcpyDeviceToHost,
+                            s) != cudaSuccess)
+          st = MOFFT_INTERNAL_ERROR;
+      }
+      for (int i = 0; i < 2; ++i)
+        if (cudaStreamSynchronize(streams[i]) != cudaSuccess && st == MOFFT_SUCCESS)
+          st = MOFFT_INTERNAL_ERROR;
       if (st != MOFFT_SUCCESS) cudaGetLastError();
       if (st == MOFFT_SUCCESS && c->form != 0) st = mofft_core_check_status(c);
     }

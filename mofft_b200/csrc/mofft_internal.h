@@ -71,6 +71,8 @@ typedef struct mofft_core {
   void *stream;            /* plan-owned cudaStream_t */
   void *user_stream;       /* attached cudaStream_t, or NULL */
   void *d_stage[2];        /* host-pointer staging buffers (lazy) */
+  void *stream2;           /* second plan-owned stream of the host-buffer
+                              pipeline (lazy) */
   size_t stage_bytes;
   pthread_mutex_t lock;
 } mofft_core;
