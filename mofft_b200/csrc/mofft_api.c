@@ -995,12 +995,12 @@ mofft_status mofft_core_execute(const mofft_core *cc, const void *in, void *out)
     pthread_mutex_lock(&c->lock);
     st = ensure_staging(c);
     if (st == MOFFT_SUCCESS) {
-      /* Chunks of about 64 MiB alternate between two streams, so the upload
+      /* Chunks of about 24 MiB alternate between two streams, so the upload
        * of one chunk, the passes of another and the download of a third
        * overlap (copies from and to pinned memory run on separate engines). */
       const size_t cb = mofft_complex_bytes(c->precision_bits);
       const size_t span = ((c->batch - 1) * c->distance + c->length) * cb;
-      const size_t chunk_bytes = (size_t)64 << 20;
+      const size_t chunk_bytes = (size_t)24 << 20;
       size_t chunks = (span + chunk_bytes - 1) / chunk_bytes;
       if (chunks > c->batch) chunks = c->batch;
       if (chunks > 64) chunks = 64;
