@@ -352,12 +352,15 @@ struct StageRunner<T, L, TPL, NS, TWOFF, FS, LS, IS_FIRST, DTW, R, R2, Rest...> 
 // parts through the same buffer, so a line needs L words of shared memory
 // instead of 2L: twice the resident CTAs for the long one-pass lengths.
 // ---------------------------------------------------------------------------
-template <typename T, int R, int NS, int TWOFF, bool DTW, int PER, int TPL>
+// A thread runs butterflies j = t + m TPL (m < PER) of a stage with BF = L/R
+// butterflies; when TPL does not divide BF the last m is partial (j < BF).
+template <typename T, int R, int NS, int TWOFF, bool DTW, int PER, int TPL, int BF>
 __device__ __forceinline__ void split_compute(T (&vr)[PER][R], T (&vi)[PER][R], int t,
                                               const cplx_t<T>* __restrict__ tw) {
 #pragma unroll
   for (int m = 0; m < PER; ++m) {
     const int j = t + m * TPL;
+    if (BF % TPL != 0 && j >= BF) continue;
     if (NS > 1) {
       const int jm = j % NS;
       if constexpr (DTW && R == 16) {
@@ -375,11 +378,12 @@ __device__ __forceinline__ void split_compute(T (&vr)[PER][R], T (&vi)[PER][R], 
 }
 
 // Stockham output positions of stage (R, NS): y[(j/NS) NS R + j%NS + k NS].
-template <typename T, int R, int NS, int PER, int TPL>
+template <typename T, int R, int NS, int PER, int TPL, int BF>
 __device__ __forceinline__ void split_put(T* buf, const T (&v)[PER][R], int t) {
 #pragma unroll
   for (int m = 0; m < PER; ++m) {
     const int j = t + m * TPL;
+    if (BF % TPL != 0 && j >= BF) continue;
     const int base = (j / NS) * NS * R + (j % NS);
 #pragma unroll
     for (int k = 0; k < R; ++k) buf[spad<T>(base + k * NS)] = v[m][k];
@@ -393,6 +397,7 @@ __device__ __forceinline__ void split_get(const T* buf, T (&v)[PER][R], int t) {
 #pragma unroll
   for (int m = 0; m < PER; ++m) {
     const int j = t + m * TPL;
+    if (BF % TPL != 0 && j >= BF) continue;
 #pragma unroll
     for (int r = 0; r < R; ++r) v[m][r] = buf[spad<T>(j + r * BF)];
   }
@@ -400,16 +405,17 @@ __device__ __forceinline__ void split_get(const T* buf, T (&v)[PER][R], int t) {
 
 template <typename T, int L, int TPL, int NS, int TWOFF, bool DTW, int R, int... Rest>
 struct SplitRunner {
-  static constexpr int PER = (L / R) / TPL;
-  static_assert((L / R) % TPL == 0, "split exchange needs whole butterflies per thread");
+  static constexpr int BF = L / R;
+  static constexpr int PER = (BF + TPL - 1) / TPL;
   __device__ __forceinline__ static void run(T* buf, const RowsLayout<T>& lay, int t,
                                              const cplx_t<T>* tw, T (&vr)[PER][R],
                                              T (&vi)[PER][R]) {
-    split_compute<T, R, NS, TWOFF, DTW, PER, TPL>(vr, vi, t, tw);
+    split_compute<T, R, NS, TWOFF, DTW, PER, TPL, BF>(vr, vi, t, tw);
     if constexpr (sizeof...(Rest) == 0) {
 #pragma unroll
       for (int m = 0; m < PER; ++m) {
         const int j = t + m * TPL;
+        if (BF % TPL != 0 && j >= BF) continue;
         const int base = (j / NS) * NS * R + (j % NS);
 #pragma unroll
         for (int k = 0; k < R; ++k) lay.gstore(base + k * NS, vr[m][k], vi[m][k]);
@@ -419,11 +425,11 @@ struct SplitRunner {
       constexpr int R2 = Next::kRadix;
       T nr[Next::PER][R2];
       T ni[Next::PER][R2];
-      split_put<T, R, NS, PER, TPL>(buf, vr, t);
+      split_put<T, R, NS, PER, TPL, BF>(buf, vr, t);
       __syncthreads();
       split_get<T, L, R2, Next::PER, TPL>(buf, nr, t);
       __syncthreads();
-      split_put<T, R, NS, PER, TPL>(buf, vi, t);
+      split_put<T, R, NS, PER, TPL, BF>(buf, vi, t);
       __syncthreads();
       split_get<T, L, R2, Next::PER, TPL>(buf, ni, t);
       __syncthreads();
@@ -445,6 +451,7 @@ __device__ __forceinline__ void rows_body_split(const RowsLayout<T>& lay, T* buf
 #pragma unroll
   for (int m = 0; m < First::PER; ++m) {
     const int j = t + m * TPL;
+    if (BF % TPL != 0 && j >= BF) continue;
 #pragma unroll
     for (int r = 0; r < R0; ++r) lay.gload(j + r * BF, vr[m][r], vi[m][r]);
   }

@@ -219,6 +219,9 @@ struct GenericInst {
 #define ROWSX(T, L, TPL, TB, ...) \
   RowsInst<T, L, TPL, TB, kDerivedTw | kSplitX, __VA_ARGS__>::entry( \
       "rows_" #T "_" #L "_t" #TPL "_b" #TB "_sfalse_dx")
+#define ROWSX2(T, L, TPL, TB, ...) \
+  RowsInst<T, L, TPL, TB, kDerivedTw | kSplitX | kTwoCtas, __VA_ARGS__>::entry( \
+      "rows_" #T "_" #L "_t" #TPL "_b" #TB "_sfalse_dx2")
 #define ROWSD2(T, L, TPL, TB, ...) \
   RowsInst<T, L, TPL, TB, kDerivedTw | kTwoCtas, __VA_ARGS__>::entry( \
       "rows_" #T "_" #L "_t" #TPL "_b" #TB "_sfalse_d2")

@@ -40,6 +40,19 @@ const Entry *entries_rows_mixed(int *count) {
       ROWS(double, 6144, 384, 1, false, 6, 4, 16, 16),
       ROWS(double, 10240, 640, 1, false, 5, 8, 16, 16),
       ROWS(double, 12288, 768, 1, false, 3, 16, 16, 16),
+      // split exchanges (one component per exchange: half the shared memory)
+      ROWSX(double, 2560, 160, 1, 10, 16, 16),
+      ROWSX(double, 3072, 192, 1, 12, 16, 16),
+      ROWSX(double, 5120, 320, 1, 5, 4, 16, 16),
+      ROWSX(double, 6144, 384, 1, 6, 4, 16, 16),
+      ROWSX2(double, 2560, 160, 1, 10, 16, 16),
+      ROWSX2(double, 3072, 192, 1, 12, 16, 16),
+      ROWSX2(double, 5120, 320, 1, 5, 4, 16, 16),
+      ROWSX2(double, 6144, 384, 1, 6, 4, 16, 16),
+      ROWSX(float, 5120, 320, 1, 5, 4, 16, 16),
+      ROWSX(float, 6144, 384, 1, 6, 4, 16, 16),
+      ROWSX(float, 10240, 640, 1, 5, 8, 16, 16),
+      ROWSX(float, 12288, 768, 1, 3, 16, 16, 16),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;
