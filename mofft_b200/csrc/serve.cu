@@ -195,14 +195,6 @@ mofft_status launch_group(mofft_server *S, int idx) {
       post.push_back({q->r.output, b.ptr, bytes,
                       q->host_out ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice});
       dout = static_cast<unsigned char *>(b.ptr);
-    } else if (in_place && q->host_in) {
-      dout = const_cast<unsigned char *>(din);   // one-pass in place on the staging copy
-      Block b;
-      (void)b;
-    }
-    if (in_place && q->host_in && !(q->host_out || two_pass)) {
-      // result lands in the staging block; copy it back to the host buffer
-      post.push_back({q->r.output, din, bytes, cudaMemcpyDeviceToHost});
     }
     for (size_t t = 0; t < q->r.batch; ++t, ++k) {
       st.h_table[k] = const_cast<unsigned char *>(din) + t * n * eb;
