@@ -36,6 +36,23 @@ mofft_status mofft_plan_create_batched_with_radices_f64(
     mofft_direction direction, mofft_placement placement, const int *radices,
     size_t radix_count);
 
+/* Batched plan with an explicit kernel per pass: `kernels` holds `count`
+ * registry indices (mofft_kernel_info), first pass first -- one one-pass
+ * (kind 0) kernel, or two to four column-pass (kind 1) kernels whose line
+ * lengths multiply to `length`.  The plan runs exactly those kernels (the
+ * tuned variants the autotuner chooses between, e.g. for tests or for
+ * replaying a measurement); the kernels' radix lists form the plan's chain.
+ * MOFFT_INVALID_ARGUMENT for kernels that do not form such a schedule,
+ * MOFFT_UNSUPPORTED_SIZE if the schedule cannot be built. */
+mofft_status mofft_plan_create_batched_with_kernels_f32(
+    mofft_plan_f32 **plan, size_t length, size_t batch, size_t distance,
+    mofft_direction direction, mofft_placement placement, const int *kernels,
+    size_t count);
+mofft_status mofft_plan_create_batched_with_kernels_f64(
+    mofft_plan_f64 **plan, size_t length, size_t batch, size_t distance,
+    mofft_direction direction, mofft_placement placement, const int *kernels,
+    size_t count);
+
 /* `stream` is a cudaStream_t (NULL = blocking calls on a plan-owned stream). */
 mofft_status mofft_plan_set_stream_f32(mofft_plan_f32 *plan, void *stream);
 mofft_status mofft_plan_set_stream_f64(mofft_plan_f64 *plan, void *stream);

@@ -159,6 +159,8 @@ _TYPED = [
       ctypes.POINTER(Diagnostics)]),
     ("mofft_plan_create_batched_with_radices_{s}", _I,
      [ctypes.POINTER(_P), _SZ, _SZ, _SZ, _I, _I, ctypes.POINTER(_I), _SZ]),
+    ("mofft_plan_create_batched_with_kernels_{s}", _I,
+     [ctypes.POINTER(_P), _SZ, _SZ, _SZ, _I, _I, ctypes.POINTER(_I), _SZ]),
     ("mofft_plan_set_stream_{s}", _I, [_P, _P]),
     ("mofft_plan_get_batch_{s}", _I, [_P, ctypes.POINTER(_SZ), ctypes.POINTER(_SZ)]),
     ("mofft_plan_get_schedule_{s}", _I, [_P, ctypes.POINTER(Schedule)]),
@@ -323,11 +325,17 @@ class Plan:
                *, bits: int = 32, batch: int = 1, distance: int = 0,
                mode: int = PLANNER_PRETUNED, flags: int = 0, candidate_limit: int = 0,
                timing_samples: int = 0, radices: Optional[Sequence[int]] = None,
+               kernels: Optional[Sequence[int]] = None,
                diagnostics: Optional[Diagnostics] = None) -> "Plan":
         lib = load()
         s = "f32" if bits == 32 else "f64"
         h = ctypes.c_void_p()
-        if radices is not None:
+        if kernels is not None:
+            arr = _int_array(kernels)
+            st = getattr(lib, f"mofft_plan_create_batched_with_kernels_{s}")(
+                ctypes.byref(h), length, batch, distance, direction, placement, arr,
+                len(kernels))
+        elif radices is not None:
             arr = _int_array(radices)
             st = getattr(lib, f"mofft_plan_create_batched_with_radices_{s}")(
                 ctypes.byref(h), length, batch, distance, direction, placement, arr,

@@ -485,6 +485,48 @@ static int options_from_bound_flags(uint32_t flags, mofft_plan_options *o) {
 
 #define CORE(p) (&(p)->core)
 
+/* Plan whose schedule runs exactly `kernels` (registry indices, one per pass,
+ * first pass first); the kernels' in-CTA radix lists, concatenated, are the
+ * plan's chain. */
+static mofft_status create_with_kernels(mofft_core **out, int precision_bits,
+                                        size_t length, size_t batch, size_t distance,
+                                        mofft_direction direction,
+                                        mofft_placement placement, const int *kernels,
+                                        size_t count) {
+  if (!kernels || count == 0 || count > MOFFT_MAX_PASSES || !valid_shape(direction, placement))
+    return MOFFT_INVALID_ARGUMENT;
+  int chain[MOFFT_MAX_STAGES];
+  int preferred[MOFFT_MAX_PASSES];
+  int depth = 0;
+  size_t product = 1;
+  for (int i = 0; i < MOFFT_MAX_PASSES; ++i) preferred[i] = -1;
+  for (size_t p = 0; p < count; ++p) {
+    const mofft_kernel_desc *d = mofft_cuda_kernel_get(kernels[p]);
+    if (!d || d->precision_bits != precision_bits ||
+        d->kind != (count == 1 ? MOFFT_KERNEL_ROWS : MOFFT_KERNEL_COLS) ||
+        d->radix_count <= 0 || depth + d->radix_count > MOFFT_MAX_STAGES)
+      return MOFFT_INVALID_ARGUMENT;
+    memcpy(chain + depth, d->radices, (size_t)d->radix_count * sizeof(int));
+    depth += d->radix_count;
+    product *= (size_t)d->length;
+    preferred[p] = kernels[p];
+  }
+  if (product != length) return MOFFT_INVALID_ARGUMENT;
+  if (!mofft_hardware_supports(precision_bits)) return MOFFT_UNSUPPORTED_HARDWARE;
+  mofft_status st = mofft_core_create_tuned(out, precision_bits, length, batch, distance,
+                                            direction, placement, chain, depth, preferred);
+  if (st != MOFFT_SUCCESS) return st;
+  const mofft_core *c = *out;
+  int ok = c->sched.pass_count == (int)count;
+  for (size_t p = 0; ok && p < count; ++p) ok = c->sched.pass[p].kernel == kernels[p];
+  if (!ok) {
+    mofft_core_destroy(*out);
+    *out = NULL;
+    return MOFFT_UNSUPPORTED_SIZE;
+  }
+  return MOFFT_SUCCESS;
+}
+
 #define DEFINE_TYPED_API(SUF, BITS, PLAN, CPLX)                                  \
   mofft_status mofft_plan_create_##SUF(PLAN **out, size_t length,                \
                                        mofft_direction direction,                \
@@ -540,6 +582,17 @@ static int options_from_bound_flags(uint32_t flags, mofft_plan_options *o) {
     return create_with_radices((mofft_core **)out, BITS, length, batch,         \
                                distance, direction, placement, radices,          \
                                radix_count);                                     \
+  }                                                                              \
+  mofft_status mofft_plan_create_batched_with_kernels_##SUF(                     \
+      PLAN **out, size_t length, size_t batch, size_t distance,                  \
+      mofft_direction direction, mofft_placement placement,                      \
+      const int *kernels, size_t count) {                                        \
+    if (!out) return MOFFT_INVALID_ARGUMENT;                                     \
+    *out = NULL;                                                                 \
+    if (batch == 0 || (distance != 0 && distance < length))                      \
+      return MOFFT_INVALID_ARGUMENT;                                             \
+    return create_with_kernels((mofft_core **)out, BITS, length, batch,         \
+                               distance, direction, placement, kernels, count);  \
   }                                                                              \
   PLAN *mofft_plan_dft_1d_##SUF(size_t length, const CPLX *input, CPLX *output,  \
                                 mofft_direction direction, uint32_t flags) {     \

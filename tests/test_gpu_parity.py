@@ -23,13 +23,13 @@ CTYPE = {32: np.complex64, 64: np.complex128}
 
 
 def run_host(x: np.ndarray, direction: int, *, bits: int, inplace: bool = False,
-             radices=None, bank: int = 0) -> np.ndarray:
+             radices=None, bank: int = 0, kernels=None) -> np.ndarray:
     """Execute through the C-ABI with host (numpy) buffers."""
     x = np.ascontiguousarray(x, dtype=CTYPE[bits])
     n = x.shape[-1]
     batch = x.size // n
     with m.Plan.create(n, direction, m.IN_PLACE if inplace else m.OUT_OF_PLACE, bits=bits,
-                       batch=batch, radices=radices) as plan:
+                       batch=batch, radices=radices, kernels=kernels) as plan:
         if bank:
             plan.set_kernel_bank(bank)
         if inplace:
@@ -246,19 +246,21 @@ def test_sweep_in_place_sampled(n):
 
 
 def test_every_specialised_kernel():
-    """Each compiled specialised kernel, forced through its exact radix chain,
-    against the oracle (odd batch to exercise tail CTAs)."""
+    """Each compiled one-pass kernel (every variant, selected by registry
+    index) against the oracle, both directions, in and out of place, odd
+    batch to exercise tail CTAs."""
     ks = [k for k in m.kernels() if k["kind"] == m.KERNEL_ROWS]
     for k in ks:
         n = k["length"]
-        chain = list(reversed(k["radices"]))
         batch = 7
         x = oracle.uniform(n * batch, seed=99, dtype=CTYPE[k["precision_bits"]]).reshape(batch, n)
+        tol = fp32_tol(n) if k["precision_bits"] == 32 else fp64_tol(n)
         for direction in (-1, 1):
-            y = run_host(x, direction, bits=k["precision_bits"], radices=chain)
             ref = oracle.fft_ld(x.astype(np.complex128), direction)
-            tol = fp32_tol(n) if k["precision_bits"] == 32 else fp64_tol(n)
-            assert rel_l2(y, ref) <= tol, k["name"]
+            for inplace in (False, True):
+                y = run_host(x, direction, bits=k["precision_bits"], kernels=[k["index"]],
+                             inplace=inplace)
+                assert rel_l2(y, ref) <= tol, (k["name"], direction, inplace)
 
 
 def test_batch_distance_and_stream():
@@ -295,39 +297,45 @@ def test_torch_convenience_matches_oracle():
     assert rel_l2(y.cpu().numpy(), oracle.fft_ld(x.numpy(), -1)) <= fp64_tol(512)
 
 
-def _cols_cover_case(k):
-    """A radix chain (reference order) whose canonical two-pass schedule runs
-    column kernel k, found with the host-side schedule preview."""
-    bits = k["precision_bits"]
-    for e in range(4, 13):
-        partner = [16] * (e // 4) + ([2 ** (e % 4)] if e % 4 else [])
-        for stockham in (k["radices"] + partner, partner + k["radices"]):
-            n = int(np.prod(stockham))
+def _cols_partners(k, ks):
+    """Two-pass schedules (kernel indices) that run column kernel k, once as
+    the first pass and once as the second where some partner allows it."""
+    out = []
+    same = [p for p in ks if p["precision_bits"] == k["precision_bits"]]
+    for first in (True, False):
+        for p in sorted(same, key=lambda q: q["length"]):
+            pair = [k, p] if first else [p, k]
+            n = pair[0]["length"] * pair[1]["length"]
+            if n > (1 << 20):
+                continue
             try:
-                s = m.schedule_preview(n, bits, radices=list(reversed(stockham)))
+                with m.Plan.create(n, m.FORWARD, m.OUT_OF_PLACE, bits=k["precision_bits"],
+                                   kernels=[q["index"] for q in pair]):
+                    pass
             except m.MofftError:
                 continue
-            if s["pass_count"] == 2 and k["index"] in s["kernels"]:
-                return n, list(reversed(stockham))
-    return None
+            out.append((n, [q["index"] for q in pair]))
+            break
+    return out
 
 
 def test_every_column_kernel():
-    """Each compiled column-pass kernel inside a two-pass plan, against the
-    oracle, both directions, odd batch."""
+    """Each compiled column-pass kernel (every variant, selected by registry
+    index) inside two-pass plans -- as the first pass and as the second --
+    against the oracle, both directions, odd batch."""
     ks = [k for k in m.kernels() if k["kind"] == m.KERNEL_COLS]
     missing = []
     for k in ks:
-        case = _cols_cover_case(k)
-        if case is None:
+        cases = _cols_partners(k, ks)
+        if not cases:
             missing.append(k["name"])
             continue
-        n, radices = case
-        batch = 3
-        x = oracle.uniform(n * batch, seed=n, dtype=CTYPE[k["precision_bits"]]).reshape(batch, n)
-        for direction in (-1, 1):
-            y = run_host(x, direction, bits=k["precision_bits"], radices=radices)
-            ref = oracle.fft_ld(x.astype(np.complex128), direction)
+        for n, kernels in cases:
+            batch = 3
+            x = oracle.uniform(n * batch, seed=n, dtype=CTYPE[k["precision_bits"]]).reshape(batch, n)
             tol = fp32_tol(n) if k["precision_bits"] == 32 else fp64_tol(n)
-            assert rel_l2(y, ref) <= tol, (k["name"], n, radices)
+            for direction in (-1, 1):
+                y = run_host(x, direction, bits=k["precision_bits"], kernels=kernels)
+                ref = oracle.fft_ld(x.astype(np.complex128), direction)
+                assert rel_l2(y, ref) <= tol, (k["name"], n, kernels)
     assert not missing, missing

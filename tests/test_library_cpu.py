@@ -196,6 +196,28 @@ def test_kernel_registry_is_consistent():
                        k["precision_bits"] == bits for k in ks), (bits, n)
 
 
+def test_explicit_kernel_plans_validate_before_hardware():
+    lib = m.load()
+    ks = m.kernels()
+    rows = {(k["precision_bits"], k["length"]): k["index"] for k in ks
+            if k["kind"] == m.KERNEL_ROWS}
+    cols = [k for k in ks if k["kind"] == m.KERNEL_COLS and k["precision_bits"] == 32]
+    h = ctypes.c_void_p(1)
+
+    def make(bits, n, idx):
+        arr = (ctypes.c_int * len(idx))(*idx)
+        fn = getattr(lib, f"mofft_plan_create_batched_with_kernels_f{bits}")
+        return fn(ctypes.byref(h), n, 4, 0, m.FORWARD, m.OUT_OF_PLACE, arr, len(idx))
+
+    assert make(32, 4096, [rows[(64, 4096)]]) == m.Status.INVALID_ARGUMENT   # precision
+    assert make(32, 2048, [rows[(32, 4096)]]) == m.Status.INVALID_ARGUMENT   # length
+    assert make(32, 4096, [cols[0]["index"]]) == m.Status.INVALID_ARGUMENT   # one COLS pass
+    assert make(32, 4096, [-1]) == m.Status.INVALID_ARGUMENT
+    assert h.value is None
+    if not cuda_available():
+        assert make(32, 4096, [rows[(32, 4096)]]) == m.Status.UNSUPPORTED_HARDWARE
+
+
 def test_tensor_forms_registered_and_never_planned():
     ks = m.kernels()
     tensor = sorted((k["name"], k["length"], k["radices"], k["precision_bits"])
