@@ -135,6 +135,14 @@ mofft_status launch_group(mofft_server *S, int idx) {
   const size_t eb = elem_bytes(head.precision_bits);
   const size_t n = head.length;
   const bool two_pass = plan->sched.pass_count > 1;
+  // Runtime-stage (generic) kernels take no pointer tables: such a group runs
+  // one plain batched launch per request on the same stream.
+  bool tables = true;
+  for (int p = 0; p < plan->sched.pass_count; ++p)
+    if (plan->sched.pass[p].kind != MOFFT_KERNEL_ROWS &&
+        plan->sched.pass[p].kind != MOFFT_KERNEL_COLS)
+      tables = false;
+  if (!tables && plan->sched.pass_count > 2) return MOFFT_UNSUPPORTED_SIZE;
   if (st.group.size() == 1) {
     const Req *q = st.group.front();
     const bool in_place = q->r.input == q->r.output;
@@ -196,19 +204,26 @@ mofft_status launch_group(mofft_server *S, int idx) {
                       q->host_out ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice});
       dout = static_cast<unsigned char *>(b.ptr);
     }
+    if (!tables) {
+      status = mofft_core_enqueue_batch(plan, din, dout, q->r.batch, n, st.s);
+      if (status != MOFFT_SUCCESS) return status;
+      continue;
+    }
     for (size_t t = 0; t < q->r.batch; ++t, ++k) {
       st.h_table[k] = const_cast<unsigned char *>(din) + t * n * eb;
       st.h_table[st.table_cap + k] = dout + t * n * eb;
     }
   }
-  if (cudaMemcpyAsync(st.d_table, st.h_table, k * sizeof(void *), cudaMemcpyHostToDevice,
-                      st.s) != cudaSuccess ||
-      cudaMemcpyAsync(st.d_table + st.table_cap, st.h_table + st.table_cap,
-                      k * sizeof(void *), cudaMemcpyHostToDevice, st.s) != cudaSuccess)
-    return MOFFT_INTERNAL_ERROR;
-  status = mofft_core_enqueue_indirect(plan, st.d_table, st.d_table + st.table_cap,
-                                       (long long)transforms, st.s);
-  if (status != MOFFT_SUCCESS) return status;
+  if (tables) {
+    if (cudaMemcpyAsync(st.d_table, st.h_table, k * sizeof(void *), cudaMemcpyHostToDevice,
+                        st.s) != cudaSuccess ||
+        cudaMemcpyAsync(st.d_table + st.table_cap, st.h_table + st.table_cap,
+                        k * sizeof(void *), cudaMemcpyHostToDevice, st.s) != cudaSuccess)
+      return MOFFT_INTERNAL_ERROR;
+    status = mofft_core_enqueue_indirect(plan, st.d_table, st.d_table + st.table_cap,
+                                         (long long)transforms, st.s);
+    if (status != MOFFT_SUCCESS) return status;
+  }
   for (const Post &p : post)
     if (cudaMemcpyAsync(p.dst, p.src, p.bytes, p.kind, st.s) != cudaSuccess)
       return MOFFT_INTERNAL_ERROR;

@@ -103,3 +103,31 @@ def test_admission_cap():
     with pytest.raises(m.MofftError):
         srv.submit(17 * 16, 1, -1, 32, x.data_ptr(), y.data_ptr())
     srv.destroy()
+
+
+def test_lengths_on_runtime_stage_kernels():
+    """A length without a specialised kernel (7 * 64 = 448, 11 * 1024 = 11264)
+    runs on the runtime-stage kernels, which take no pointer tables: several
+    such requests waiting together still complete correctly (one plain
+    launch each), on host and on device buffers."""
+    import torch
+    srv = m.Server(streams=2)
+    reqs = []
+    for k, (n, bits) in enumerate([(448, 32), (448, 32), (11264, 64), (11264, 64), (448, 64)]):
+        x = _tensor(3, n, bits, 100 + k)
+        if k % 2:
+            hx = x.cpu().pin_memory()
+            hy = torch.empty_like(hx).pin_memory()
+            reqs.append((srv.submit(n, 3, -1, bits, hx.data_ptr(), hy.data_ptr()), x, hy, n,
+                         bits, hx))
+        else:
+            y = torch.empty_like(x)
+            reqs.append((srv.submit(n, 3, -1, bits, x.data_ptr(), y.data_ptr()), x, y, n,
+                         bits, None))
+    for t, x, y, n, bits, _ in reqs:
+        st, _lat = srv.wait(t)
+        assert st == 0, (n, bits)
+        torch.cuda.synchronize()
+        ref = oracle.fft_ld(x.cpu().numpy().astype(np.complex128), -1)
+        assert rel_l2(y.cpu().numpy(), ref) <= (fp32_tol(n) if bits == 32 else fp64_tol(n))
+    srv.destroy()
