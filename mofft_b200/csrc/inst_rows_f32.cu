@@ -33,6 +33,12 @@ const Entry *entries_rows_f32(int *count) {
       ROWSD(float, 4096, 512, 1, false, 16, 16, 16),
       ROWSD(float, 8192, 512, 1, false, 16, 16, 16, 2),
       ROWSD(float, 16384, 512, 1, false, 16, 16, 16, 4),
+      // more or fewer points per thread for the small staged lengths
+      ROWS(float, 32, 2, 128, true, 16, 2),
+      ROWS(float, 64, 2, 128, true, 16, 4),
+      ROWS(float, 64, 8, 32, true, 8, 8),
+      ROWS(float, 128, 4, 64, true, 16, 8),
+      ROWS(float, 128, 16, 16, true, 8, 16),
       // radix-32 stages: one exchange fewer for the long lines
       ROWSD2(float, 8192, 256, 1, 32, 16, 16),
       ROWSD2(float, 8192, 256, 1, 16, 16, 32),

@@ -20,6 +20,9 @@ const Entry *entries_rows_f64(int *count) {
       ROWS(double, 4096, 256, 1, false, 16, 16, 16),
       ROWS(double, 4096, 512, 1, false, 8, 8, 8, 8),
       ROWS(double, 8192, 512, 1, false, 16, 16, 16, 2),
+      ROWS(double, 64, 4, 32, true, 16, 4),
+      ROWS(double, 128, 8, 16, true, 16, 8),
+      ROWS(double, 32, 2, 64, true, 16, 2),
       ROWSD(double, 1024, 64, 2, false, 16, 16, 4),
       ROWSD(double, 4096, 256, 1, false, 16, 16, 16),
       ROWSD(double, 8192, 512, 1, false, 16, 16, 16, 2),
