@@ -122,6 +122,7 @@ typedef struct {
 typedef struct mofft_plan_f32 mofft_plan_f32;
 typedef struct mofft_plan_f64 mofft_plan_f64;
 
+/* Replaces include/mofft.h:107-113 (implementation src/mofft.c:1232-1280). */
 mofft_status mofft_plan_create_f32(mofft_plan_f32 **plan, size_t length,
                                    mofft_direction direction,
                                    mofft_placement placement);
@@ -129,7 +130,8 @@ mofft_status mofft_plan_create_f64(mofft_plan_f64 **plan, size_t length,
                                    mofft_direction direction,
                                    mofft_placement placement);
 
-/* Fills PRETUNED defaults; a NULL options pointer means the same. */
+/* Fills PRETUNED defaults; a NULL options pointer means the same.
+ * Replaces include/mofft.h:116-127 (src/mofft.c:739-762, 1282-1382). */
 void mofft_plan_options_init(mofft_plan_options *options);
 mofft_status mofft_plan_create_with_options_f32(
     mofft_plan_f32 **plan, size_t length, mofft_direction direction,
@@ -140,7 +142,8 @@ mofft_status mofft_plan_create_with_options_f64(
     mofft_placement placement, const mofft_plan_options *options,
     mofft_plan_diagnostics *diagnostics);
 
-/* Bound-array lifecycle: NULL on failure; flags are 0, MOFFT_FLAG_MEASURE or
+/* Replaces include/mofft.h:129-136 (src/mofft.c:1384-1442).
+ * Bound-array lifecycle: NULL on failure; flags are 0, MOFFT_FLAG_MEASURE or
  * MOFFT_FLAG_WISDOM_ONLY.  Placement follows input == output and the plan
  * keeps both addresses for mofft_execute_plan_*. */
 mofft_plan_f32 *mofft_plan_dft_1d_f32(
@@ -152,7 +155,8 @@ mofft_plan_f64 *mofft_plan_dft_1d_f64(
 mofft_status mofft_execute_plan_f32(const mofft_plan_f32 *plan);
 mofft_status mofft_execute_plan_f64(const mofft_plan_f64 *plan);
 
-/* Explicit radix chain, outermost level first (the last radix is the first
+/* Replaces include/mofft.h:140-145 (src/mofft.c:1054-1080, 1444-1470).
+ * Explicit radix chain, outermost level first (the last radix is the first
  * stage applied).  Every radix must be one of 2..16, 32, 64 and the product
  * must equal length. */
 mofft_status mofft_plan_create_with_radices_f32(
@@ -161,7 +165,8 @@ mofft_status mofft_plan_create_with_radices_f32(
 mofft_status mofft_plan_create_with_radices_f64(
     mofft_plan_f64 **plan, size_t length, mofft_direction direction,
     mofft_placement placement, const int *radices, size_t radix_count);
-/* Layout knobs of the reference's CPU driver.  They are validated, kept, and
+/* Replaces include/mofft.h:147-171 (src/mofft.c:1498-1598).
+ * Layout knobs of the reference's CPU driver.  They are validated, kept, and
  * exported in recipes; on the GPU every level exchange happens inside shared
  * memory, so they do not change the result. */
 mofft_status mofft_plan_set_transpose_strategy_f32(
@@ -191,7 +196,8 @@ mofft_status mofft_plan_get_kernel_bank_f32(const mofft_plan_f32 *plan,
 mofft_status mofft_plan_get_kernel_bank_f64(const mofft_plan_f64 *plan,
                                              unsigned int *bank);
 
-/* 64 lowercase hex digits identifying this build (kernels, planner, wisdom).
+/* Replaces include/mofft.h:176-194 (src/mofft.c:1600-1842).
+ * 64 lowercase hex digits identifying this build (kernels, planner, wisdom).
  * Recipes are text records scoped to the build and the GPU family (compute
  * capability and SM count); they hold no pointers or timings. */
 const char *mofft_build_id(void);
@@ -212,6 +218,7 @@ mofft_status mofft_plan_import_f64(mofft_plan_f64 **plan, const char *recipe,
                                    size_t recipe_size,
                                    mofft_plan_diagnostics *diagnostics);
 
+/* Replaces include/mofft.h:196-203 (src/mofft.c:2169-2211). */
 mofft_status mofft_execute_f32(const mofft_plan_f32 *plan,
                                const mofft_complex_f32 *input,
                                mofft_complex_f32 *output);
@@ -221,7 +228,8 @@ mofft_status mofft_execute_f64(const mofft_plan_f64 *plan,
 
 void mofft_plan_destroy_f32(mofft_plan_f32 *plan);
 void mofft_plan_destroy_f64(mofft_plan_f64 *plan);
-/* Analytical cost model (B200 parameters: HBM / L2 bandwidth, FP32 / FP64
+/* Replaces include/mofft.h:205-227 (src/mofft.c:133-325, 2213-2218).
+ * Analytical cost model (B200 parameters: HBM / L2 bandwidth, FP32 / FP64
  * throughput, 128-byte lines), in microseconds. */
 double mofft_estimated_radix_cost(int radix, int precision_bits,
                                   int first_stage);
@@ -240,6 +248,7 @@ mofft_status mofft_estimated_plan_cost_breakdown_with_layout(
     size_t length, int precision_bits, const int *radices, size_t radix_count,
     uint64_t blocked_transpose_mask, int direct_input,
     mofft_stage_layout layout, mofft_plan_cost_breakdown *breakdown);
+/* Replaces include/mofft.h:228-231 (src/mofft.c:2219-2242). */
 int mofft_wisdom_is_formal(void);
 const char *mofft_wisdom_source(void);
 const char *mofft_status_string(mofft_status status);
