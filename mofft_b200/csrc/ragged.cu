@@ -107,7 +107,6 @@ constexpr int kArgCount = (int)sizeof...(R);
    ColsGeom<float, L, TPL, kColsLines>::SMEM},
 
 const ConfigInfo kConfigs[] = {MOFFT_RAGGED_ROWS(MOFFT_ROWS_INFO) MOFFT_RAGGED_COLS(MOFFT_COLS_INFO)};
-constexpr int kConfigCount = (int)(sizeof(kConfigs) / sizeof(kConfigs[0]));
 
 __device__ __forceinline__ RowsArgs<float> rows_args_of(const RItem &it) {  // NOLINT
   RowsArgs<float> a;
