@@ -61,7 +61,8 @@ struct RTile {
 };
 
 // Single-pass configurations: (id, L, TPL, staged, radices...) with
-// TB = 512 / TPL transforms per tile.
+// TB = 512 / TPL transforms per tile; radix-16 stages derive their twiddles
+// from four table entries, as the tuned standalone kernels do.
 #define MOFFT_RAGGED_ROWS(X)                 \
   X(0, 64, 4, true, 16, 4)                  \
   X(1, 128, 8, true, 16, 8)                 \
@@ -161,9 +162,8 @@ __device__ __forceinline__ ColsArgs<float> cols_args_of(const RItem &it, int pas
   __device__ __noinline__ void tile_##ID(const RItem *__restrict__ itp, int pass,    \
                                          long long b, long long j0,                   \
                                          unsigned char *smem) {                       \
-    rows_body<float, L, TPL, kThreads / TPL, (ST) ? kStaged : 0, __VA_ARGS__>(           \
-        rows_args_of(*itp), b,                                                         \
-                                                              smem);                  \
+    rows_body<float, L, TPL, kThreads / TPL, ((ST) ? kStaged : 0) | kDerivedTw,          \
+              __VA_ARGS__>(rows_args_of(*itp), b, smem);                               \
   }
 #define MOFFT_COLS_FN(ID, L, TPL, ...)                                              \
   __device__ __noinline__ void tile_##ID(const RItem *__restrict__ itp, int pass,    \
