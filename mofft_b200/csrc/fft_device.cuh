@@ -352,6 +352,17 @@ struct StageRunner<T, L, TPL, NS, TWOFF, FS, LS, IS_FIRST, DTW, R, R2, Rest...> 
 // parts through the same buffer, so a line needs L words of shared memory
 // instead of 2L: twice the resident CTAs for the long one-pass lengths.
 // ---------------------------------------------------------------------------
+// Word offset of element i in a split-exchange buffer.  FP64 pads one
+// element per 32 (a bank simulation of the split exchanges of the FP64
+// lines, 2560-6144 points, gives 1.2-1.3 wavefronts per access against
+// 1.3-1.8 with the one-per-16 padding of the two-array exchanges; powers of
+// two stay conflict-free); FP32 keeps spad.
+template <typename T>
+__device__ __forceinline__ int split_pad(int i) {
+  if constexpr (sizeof(T) == 8) return i + (i >> 5);
+  else return spad<T>(i);
+}
+
 // A thread runs butterflies j = t + m TPL (m < PER) of a stage with BF = L/R
 // butterflies; when TPL does not divide BF the last m is partial (j < BF).
 template <typename T, int R, int NS, int TWOFF, bool DTW, int PER, int TPL, int BF>
@@ -386,7 +397,7 @@ __device__ __forceinline__ void split_put(T* buf, const T (&v)[PER][R], int t) {
     if (BF % TPL != 0 && j >= BF) continue;
     const int base = (j / NS) * NS * R + (j % NS);
 #pragma unroll
-    for (int k = 0; k < R; ++k) buf[spad<T>(base + k * NS)] = v[m][k];
+    for (int k = 0; k < R; ++k) buf[split_pad<T>(base + k * NS)] = v[m][k];
   }
 }
 
@@ -399,7 +410,7 @@ __device__ __forceinline__ void split_get(const T* buf, T (&v)[PER][R], int t) {
     const int j = t + m * TPL;
     if (BF % TPL != 0 && j >= BF) continue;
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[m][r] = buf[spad<T>(j + r * BF)];
+    for (int r = 0; r < R; ++r) v[m][r] = buf[split_pad<T>(j + r * BF)];
   }
 }
 
