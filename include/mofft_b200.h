@@ -114,6 +114,14 @@ mofft_status mofft_ragged_execute(mofft_ragged_plan *plan, void *stream);
 mofft_status mofft_ragged_execute_per_item(mofft_ragged_plan *plan,
                                            void *stream);
 mofft_status mofft_ragged_status(mofft_ragged_plan *plan);
+/* Failure check: runs the plan's queue once on `stream` with every
+ * second-pass dependency made unsatisfiable, so each second-pass tile gives
+ * up after its bounded wait (about a second per tile and CTA) and skips its
+ * work; mofft_ragged_status then reports MOFFT_INTERNAL_ERROR and the next
+ * mofft_ragged_execute runs normally.  Plans without two-pass items have no
+ * waits and report success.  For tests of the timeout path. */
+mofft_status mofft_ragged_check_lost_dependency(mofft_ragged_plan *plan,
+                                                void *stream);
 mofft_status mofft_ragged_plan_info(const mofft_ragged_plan *plan,
                                     size_t *tiles, int *grid);
 void mofft_ragged_plan_destroy(mofft_ragged_plan *plan);

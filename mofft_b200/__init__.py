@@ -193,6 +193,7 @@ _PLAIN = [
     ("mofft_ragged_execute", _I, [_P, _P]),
     ("mofft_ragged_execute_per_item", _I, [_P, _P]),
     ("mofft_ragged_status", _I, [_P]),
+    ("mofft_ragged_check_lost_dependency", _I, [_P, _P]),
     ("mofft_ragged_plan_info", _I, [_P, ctypes.POINTER(_SZ), ctypes.POINTER(_I)]),
     ("mofft_ragged_plan_destroy", None, [_P]),
     ("mofft_server_create", _I, [ctypes.POINTER(_P), ctypes.POINTER(ServerOptions)]),
@@ -444,6 +445,11 @@ class RaggedPlan:
 
     def status(self) -> int:
         return self._lib.mofft_ragged_status(self._h)
+
+    def check_lost_dependency(self, stream: Optional[int] = None) -> None:
+        """One run in which no second-pass dependency can be met (timeout path)."""
+        check(self._lib.mofft_ragged_check_lost_dependency(self._h, stream),
+              "ragged lost-dependency check")
 
     def info(self) -> tuple[int, int]:
         tiles = ctypes.c_size_t()

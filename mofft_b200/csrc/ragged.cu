@@ -198,7 +198,7 @@ __device__ __forceinline__ void run_tile(int cfg, const RItem *__restrict__ itp,
 // never waits, so prefetching cannot starve a dependency.
 __global__ void __launch_bounds__(kThreads, 2)
 ragged_kernel(const RItem *__restrict__ items, const RTile *__restrict__ tiles,
-              int tile_count, int *next, int *done, int *error) {
+              int tile_count, int *next, int *done, int *error, int need_bias) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_tile[2];
   __shared__ int s_skip;
@@ -214,7 +214,7 @@ ragged_kernel(const RItem *__restrict__ items, const RTile *__restrict__ tiles,
       int skip = 0;
       if (tl.pass == 1) {
         unsigned spins = 0;
-        const int need = itp->pass1_tiles;
+        const int need = itp->pass1_tiles + need_bias;
         while (atomicAdd(&done[tl.item], 0) < need) {
           if (++spins > kMaxSpins) {
             atomicExch(error, 1);
@@ -444,14 +444,14 @@ extern "C" mofft_status mofft_ragged_plan_create_f32(mofft_ragged_plan **out,
   return MOFFT_SUCCESS;
 }
 
-static cudaError_t ragged_enqueue(mofft_ragged_plan *p, cudaStream_t s) {
+static cudaError_t ragged_enqueue(mofft_ragged_plan *p, cudaStream_t s, int need_bias = 0) {
   cudaError_t e = cudaMemsetAsync(p->d_counters, 0, (p->item_count + 2) * sizeof(int), s);
   if (e != cudaSuccess) return e;
   int *next = p->d_counters;
   int *error = p->d_counters + 1;
   int *done = p->d_counters + 2;
   ragged_kernel<<<p->grid, kThreads, p->smem, s>>>(p->d_items, p->d_tiles, p->tile_count,
-                                                     next, done, error);
+                                                     next, done, error, need_bias);
   return cudaGetLastError();
 }
 
@@ -482,6 +482,21 @@ extern "C" mofft_status mofft_ragged_execute(mofft_ragged_plan *p, void *stream)
     p->graph = g;
   }
   if (cudaGraphLaunch(p->exec, s) != cudaSuccess) {
+    cudaGetLastError();
+    return MOFFT_INTERNAL_ERROR;
+  }
+  mofft_count_launches(1);
+  return MOFFT_SUCCESS;
+}
+
+// One run of the queue in which no second-pass dependency can be met: every
+// second-pass tile gives up after its bounded wait, sets the error word and
+// skips its work.  Checks that a lost dependency ends in an error status on a
+// usable context, without any GPU fault.
+extern "C" mofft_status mofft_ragged_check_lost_dependency(mofft_ragged_plan *p,
+                                                           void *stream) {
+  if (!p) return MOFFT_INVALID_ARGUMENT;
+  if (ragged_enqueue(p, static_cast<cudaStream_t>(stream), 1 << 30) != cudaSuccess) {
     cudaGetLastError();
     return MOFFT_INTERNAL_ERROR;
   }

@@ -102,3 +102,29 @@ def test_unsupported_length_rejected():
     x = torch.zeros((1, 17 * 16), dtype=torch.complex64, device="cuda")
     with pytest.raises(m.MofftError):
         m.RaggedPlan([(x, x, -1)])
+
+
+def test_lost_dependency_times_out_and_context_stays_usable():
+    """A second-pass tile whose first-pass tiles never signal gives up after
+    its bounded wait: the plan's status turns to an error, no GPU fault, and
+    the next execute of the same plan runs normally and is correct."""
+    import time
+    import torch
+    spec = [(16384, 1, -1), (256, 3, 1)]            # one two-pass item, one one-pass item
+    items = make_items(spec, seed=11)
+    plan = m.RaggedPlan([(a, b, d) for a, b, d, _ in items])
+    stream = torch.cuda.Stream()
+    t0 = time.perf_counter()
+    plan.check_lost_dependency(stream.cuda_stream)
+    stream.synchronize()
+    waited = time.perf_counter() - t0
+    assert plan.status() == m.Status.INTERNAL_ERROR
+    assert waited < 30.0, waited                       # bounded: about a second per tile
+    plan.execute(stream.cuda_stream)
+    stream.synchronize()
+    assert plan.status() == m.Status.SUCCESS
+    for (src, out, d, x) in items:
+        n = x.shape[-1]
+        ref = oracle.fft_ld(x.cpu().numpy().astype(np.complex128), d)
+        assert rel_l2(out.cpu().numpy(), ref) <= fp32_tol(n), n
+    plan.destroy()
