@@ -195,6 +195,17 @@ mofft_status mofft_plan_set_precision_form_f32(mofft_plan_f32 *plan,
 mofft_status mofft_plan_get_precision_form_f32(const mofft_plan_f32 *plan,
                                                mofft_precision_form *form);
 mofft_status mofft_plan_check_f32(mofft_plan_f32 *plan);
+/* Failure check of the tensor-core n = 4096 kernel: one launch on device
+ * buffers `input` / `output` in which the first input copy of every CTA is
+ * never issued, so each CTA's bounded wait runs out (about a second), the
+ * CTA frees its tensor memory and returns.  Returns the status an execute
+ * would then report -- MOFFT_INTERNAL_ERROR when the timeout path works --
+ * and clears the plan's error word, so the plan stays usable; `output` is
+ * left unspecified.  MOFFT_INVALID_ARGUMENT for plans that do not run that
+ * kernel.  For tests of the timeout path. */
+mofft_status mofft_plan_check_lost_copy_f32(mofft_plan_f32 *plan,
+                                            const mofft_complex_f32 *input,
+                                            mofft_complex_f32 *output);
 
 /* Kernel registry introspection.  kind: 0 one-pass rows kernel, 1 column pass
  * of a multi-pass transform, 2 generic (runtime radix list), 3 tensor-core

@@ -189,6 +189,7 @@ _PLAIN = [
     ("mofft_plan_set_precision_form_f32", _I, [_P, _I]),
     ("mofft_plan_get_precision_form_f32", _I, [_P, ctypes.POINTER(_I)]),
     ("mofft_plan_check_f32", _I, [_P]),
+    ("mofft_plan_check_lost_copy_f32", _I, [_P, _P, _P]),
     ("mofft_ragged_plan_create_f32", _I, [ctypes.POINTER(_P), ctypes.POINTER(RaggedItem), _SZ]),
     ("mofft_ragged_execute", _I, [_P, _P]),
     ("mofft_ragged_execute_per_item", _I, [_P, _P]),

@@ -749,6 +749,43 @@ static mofft_status build_tensor_schedule(mofft_core *c) {
   return materialise_schedule(c);
 }
 
+/* Failure check of the tensor-core one-pass kernel: one launch whose first
+ * input copy is never issued, so every CTA's bounded wait runs out.  Returns
+ * the status the plan then reports (MOFFT_INTERNAL_ERROR when the timeout
+ * path works) and clears the error word, so the plan stays usable. */
+mofft_status mofft_core_check_lost_copy(mofft_core *c, const void *in, void *out) {
+  if (c->sched.pass_count != 1 || c->sched.pass[0].kind != MOFFT_KERNEL_TENSOR)
+    return MOFFT_INVALID_ARGUMENT;
+  const mofft_pass *ps = &c->sched.pass[0];
+  mofft_pass_args a;
+  memset(&a, 0, sizeof(a));
+  a.in = in;
+  a.out = out;
+  a.tw = (const unsigned char *)c->d_twiddles + ps->tw_offset;
+  a.aux = (const unsigned char *)c->d_twiddles + ps->aux_offset;
+  a.status = (int *)((unsigned char *)c->d_twiddles + ps->status_offset);
+  a.batch = (long long)c->batch;
+  a.in_dist = (long long)c->distance;
+  a.out_dist = (long long)c->distance;
+  a.total = (long long)c->length;
+  a.ns_outer = 1;
+  a.length = ps->length;
+  a.lose_copy = 1;
+  cudaStream_t s = (cudaStream_t)c->stream;
+  if (mofft_cuda_launch_pass(ps->kernel, &a, s) != 0 || cudaStreamSynchronize(s) != cudaSuccess) {
+    cudaGetLastError();
+    return MOFFT_INTERNAL_ERROR;
+  }
+  atomic_fetch_add(&g_launches, 1);
+  const mofft_status observed = mofft_core_check_status(c);
+  if (cudaMemsetAsync(a.status, 0, sizeof(int), s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    cudaGetLastError();
+    return MOFFT_INTERNAL_ERROR;
+  }
+  return observed;
+}
+
 mofft_status mofft_core_check_status(const mofft_core *c) {
   for (int p = 0; p < c->sched.pass_count; ++p) {
     const mofft_pass *ps = &c->sched.pass[p];

@@ -62,6 +62,8 @@ typedef struct {
    * the kernel sets when a wait on the tensor core timed out */
   const void *aux;
   int *status;
+  int lose_copy;         /* failure check: the kernel's first copy is never
+                            issued, so its wait runs out (0 in normal use) */
   /* generic kernel only */
   int generic_cols;      /* 0 ROWS addressing, 1 COLS addressing */
   int length;            /* line length L */

@@ -42,6 +42,7 @@ mofft_status mofft_core_build(mofft_core *c);
 /* Blocking: MOFFT_INTERNAL_ERROR if a tensor-core kernel of c recorded a
  * timed-out wait, else MOFFT_SUCCESS. */
 mofft_status mofft_core_check_status(const mofft_core *c);
+mofft_status mofft_core_check_lost_copy(mofft_core *c, const void *in, void *out);
 void mofft_core_destroy(mofft_core *c);
 mofft_status mofft_core_enqueue(const mofft_core *c, const void *in, void *out,
                                 void *stream);

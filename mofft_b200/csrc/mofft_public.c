@@ -269,6 +269,19 @@ mofft_status mofft_plan_get_precision_form_f32(const mofft_plan_f32 *plan,
   return MOFFT_SUCCESS;
 }
 
+mofft_status mofft_plan_check_lost_copy_f32(mofft_plan_f32 *plan,
+                                            const mofft_complex_f32 *input,
+                                            mofft_complex_f32 *output) {
+  if (!plan || !input || !output) return MOFFT_INVALID_ARGUMENT;
+  mofft_core *c = &plan->core;
+  int saved = -1;
+  cudaGetDevice(&saved);
+  if (saved != c->device) cudaSetDevice(c->device);
+  const mofft_status st = mofft_core_check_lost_copy(c, input, output);
+  if (saved >= 0 && saved != c->device) cudaSetDevice(saved);
+  return st;
+}
+
 mofft_status mofft_plan_check_f32(mofft_plan_f32 *plan) {
   if (!plan) return MOFFT_INVALID_ARGUMENT;
   mofft_core *c = &plan->core;

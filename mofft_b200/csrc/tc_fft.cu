@@ -328,6 +328,7 @@ struct TcArgs {
   long long out_dist;
   float sign;                // -1: conjugate on load and store (backward)
   int bulk;                  // 1: inputs 16-byte aligned, bulk copies allowed
+  int lose_copy;             // failure check: the first copy is never issued
 };
 
 template <int FORM>
@@ -369,7 +370,7 @@ __global__ void __launch_bounds__(kThreads, FormTraits<FORM>::kMinBlocks)
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  if (a.bulk && tid == 0 && (long long)blockIdx.x < a.batch)
+  if (a.bulk && !a.lose_copy && tid == 0 && (long long)blockIdx.x < a.batch)
     bulk_load(in_addr, a.in + (long long)blockIdx.x * a.in_dist, kN * 8, load_bar);
 
   const int j = tid;        // this thread's butterfly = its row of A and D
@@ -550,6 +551,7 @@ struct TcInst {
     // bulk copies need 16-byte aligned sources: an aligned base and an even
     // distance (complex64 elements are 8 bytes)
     a.bulk = ((reinterpret_cast<uintptr_t>(p->in) & 15u) == 0 && (p->in_dist % 2) == 0) ? 1 : 0;
+    a.lose_copy = p->lose_copy;
     const long long grid = p->batch < resident ? p->batch : resident;
     tc_fft4096_kernel<FORM><<<(unsigned)grid, kThreads, smem(), s>>>(a);
     return cudaGetLastError();

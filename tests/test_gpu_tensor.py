@@ -216,3 +216,30 @@ def test_form_65536_schedule_and_error_ordering():
                                         for f, e in errs.items()})
     assert errs[m.FORM_FP32] <= fp32_tol(N2)
     assert errs[m.FORM_TF32X3] < errs[m.FORM_BF16X3]
+
+
+def test_lost_copy_times_out_and_plan_stays_usable():
+    """The tensor-core kernel bounds every wait: a launch whose input copies
+    are never issued ends in MOFFT_INTERNAL_ERROR after about a second per
+    CTA (no GPU fault, TMEM released), and the same plan then executes
+    correctly on the same context."""
+    import ctypes
+    import time
+    import torch
+    lib = m.load()
+    x = _mix(8, seed=21)
+    want = _expected(x, m.FORWARD)
+    d = torch.from_numpy(x).cuda()
+    out = torch.empty_like(d)
+    with m.Plan.create(N, m.FORWARD, m.OUT_OF_PLACE, bits=32, batch=8) as plan:
+        assert lib.mofft_plan_check_lost_copy_f32(plan.handle, d.data_ptr(), out.data_ptr()) \
+            == m.Status.INVALID_ARGUMENT          # CUDA-core schedule: nothing to check
+        plan.set_precision_form(m.FORM_TF32X3)
+        t0 = time.perf_counter()
+        st = lib.mofft_plan_check_lost_copy_f32(plan.handle, d.data_ptr(), out.data_ptr())
+        waited = time.perf_counter() - t0
+        assert st == m.Status.INTERNAL_ERROR
+        assert waited < 30.0, waited
+        plan.check_status()                       # the error word was cleared
+        plan.execute(d, out)
+    assert rel_l2(out.cpu().numpy(), want) <= TOL[m.FORM_TF32X3]
