@@ -382,7 +382,8 @@ class Plan:
         return v.value
 
     def check_status(self) -> None:
-        """Blocking: raises if a tensor-core kernel of this plan recorded a timeout."""
+        """Blocking: raises if a kernel of this plan that bounds its waits (tensor-core,
+        prefetching one-pass) recorded a wait that ran out."""
         if self.bits == 32:
             check(self._lib.mofft_plan_check_f32(self._h), "check")
 

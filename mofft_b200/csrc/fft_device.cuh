@@ -228,6 +228,7 @@ constexpr int kStaged = 1;       // I/O staged through shared memory
 constexpr int kDerivedTw = 2;    // radix-16 twiddles from w, w^2, w^4, w^8
 constexpr int kSplitX = 4;       // exchanges move one component at a time
 constexpr int kTwoCtas = 8;      // registers capped for two resident CTAs per SM
+constexpr int kPrefetch = 16;    // persistent CTAs; the next line arrives by bulk copy
 
 // Twiddles of one radix-16 butterfly: v[r] *= w^r.  Loads the table entries
 // of w^1, w^2, w^4 and w^8 and forms the other powers with at most three
@@ -489,6 +490,11 @@ struct RowsArgs {
   // launch serve transforms that live in unrelated buffers.
   const cplx_t<T>* const* in_table;
   cplx_t<T>* const* out_table;
+  // Prefetching kernels only: error word (may be null) that records a line
+  // copy whose bounded wait ran out, and the failure check that never issues
+  // a CTA's first copy.
+  int* status;
+  int lose_copy;
 };
 
 template <typename T>
@@ -626,6 +632,165 @@ __global__ void __launch_bounds__(TPL * TB, 2)
 rows_kernel_2cta(const RowsArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   rows_body<T, L, TPL, TB, FLAGS, Rs...>(a, (long long)blockIdx.x * TB, smem_raw);
+}
+
+// ---------------------------------------------------------------------------
+// Prefetching ROWS kernel (kPrefetch with kSplitX, one line per CTA step).
+// A long one-pass line leaves room for one or two CTAs per SM, and a CTA that
+// loads, transforms and stores its line in turn keeps HBM busy only while it
+// loads.  Here the CTAs are persistent: while a CTA transforms line b, the
+// input of its next line b + gridDim.x is already on its way into shared
+// memory by one bulk asynchronous copy (cp.async.bulk, no multicast) that
+// completes a transaction count on an mbarrier.  Shared memory holds that
+// staging line (L complex, interleaved as in global memory) and the
+// split-exchange buffer (L words).
+//
+// Every wait is bounded (kLineWaitNs of %globaltimer, or kLineWaitIters
+// polls).  When it runs out the CTA records bit kLineCopyTimedOut in the
+// status word, loads that line from global memory itself, stops prefetching
+// and, before it exits, waits once more (bounded) for the copy it issued, so
+// the output stays correct and no copy lands after the CTA has gone.
+// ---------------------------------------------------------------------------
+constexpr unsigned kLineWaitIters = 1u << 26;
+constexpr unsigned long long kLineWaitNs = 1000000000ull;  // one second
+constexpr int kLineCopyTimedOut = 4;
+
+__device__ __forceinline__ unsigned long long line_clock_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for the completion of the phase of `parity` of the mbarrier at
+// shared address `bar`; false when it gave up.
+__device__ __forceinline__ bool line_wait(uint32_t bar, uint32_t parity) {
+  const unsigned long long t0 = line_clock_ns();
+  for (unsigned it = 0; it < kLineWaitIters; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if ((it & 63u) == 63u && line_clock_ns() - t0 > kLineWaitNs) return false;
+  }
+  return false;
+}
+
+// One line into shared memory: the arrival that expects `bytes`, then the
+// bulk copy that completes them (source and destination 16-byte aligned,
+// bytes a multiple of 16).
+__device__ __forceinline__ void line_copy(uint32_t dst, const void* src, uint32_t bytes,
+                                          uint32_t bar) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+// Shared memory of a prefetching CTA: mbarrier (16 bytes), staging line,
+// split-exchange buffer.
+template <typename T, int L, int TPL>
+__host__ __device__ constexpr size_t prefetch_smem() {
+  return 16 + (size_t)L * 2 * sizeof(T) + (size_t)rows_line<T>(L, TPL, 1) * sizeof(T);
+}
+
+template <typename T, int L, int TPL, int FLAGS, int R0, int... Rs>
+__device__ __forceinline__ void rows_prefetch_body(const RowsArgs<T>& a, unsigned char* smem) {
+  static_assert(StageProduct<L, R0, Rs...>::value == L, "radices must multiply to L");
+  constexpr bool DTW = (FLAGS & kDerivedTw) != 0;
+  using First = SplitRunner<T, L, TPL, 1, 0, DTW, R0, Rs...>;
+  constexpr int BF = L / R0;
+  constexpr uint32_t kLineBytes = (uint32_t)(L * sizeof(cplx_t<T>));
+  static_assert(kLineBytes % 16 == 0, "bulk copies move multiples of 16 bytes");
+  const cplx_t<T>* stage = reinterpret_cast<const cplx_t<T>*>(smem + 16);
+  T* buf = reinterpret_cast<T*>(smem + 16 + kLineBytes);
+  const uint32_t bar = (uint32_t)__cvta_generic_to_shared(smem);
+  const uint32_t stage_addr = (uint32_t)__cvta_generic_to_shared(smem + 16);
+  const int t = threadIdx.x;
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  // Block-uniform prefetch state.
+  bool prefetching = true;   // cleared once a wait has run out
+  bool expect = false;       // line b's input is meant to be in `stage`
+  bool issued = false;       // ... and its copy was issued
+  bool stale = false;        // a copy whose wait ran out may still land
+  uint32_t parity = 0, stale_parity = 0;
+  auto start = [&](long long line, bool skip) {
+    expect = issued = false;
+    if (!prefetching || line >= a.batch) return;
+    const cplx_t<T>* src = batch_in<T>(a.in, a.in_dist, a.in_table, line);
+    if ((reinterpret_cast<uintptr_t>(src) & 15u) != 0) return;
+    expect = true;
+    if (skip) return;
+    issued = true;
+    if (t == 0) line_copy(stage_addr, src, kLineBytes, bar);
+  };
+  start(blockIdx.x, a.lose_copy != 0);
+
+  for (long long b = blockIdx.x; b < a.batch; b += gridDim.x) {
+    RowsLayout<T> lay;
+    lay.sre = buf;
+    lay.sim = buf;
+    lay.active = true;
+    lay.gin = batch_in<T>(a.in, a.in_dist, a.in_table, b);
+    lay.gout = batch_out<T>(a.out, a.out_dist, a.out_table, b);
+    lay.sign = a.sign;
+    T vr[First::PER][R0];
+    T vi[First::PER][R0];
+    bool landed = expect ? line_wait(bar, parity) : true;
+    landed = __syncthreads_and(landed) != 0;
+    if (expect && landed) {
+      parity ^= 1u;
+#pragma unroll
+      for (int m = 0; m < First::PER; ++m) {
+        const int j = t + m * TPL;
+        if (BF % TPL != 0 && j >= BF) continue;
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+          const cplx_t<T> v = stage[j + r * BF];
+          vr[m][r] = v.x;
+          vi[m][r] = v.y * a.sign;
+        }
+      }
+    } else {
+      if (expect) {
+        if (t == 0 && a.status) atomicOr(a.status, kLineCopyTimedOut);
+        prefetching = false;
+        stale = issued;
+        stale_parity = parity;
+      }
+#pragma unroll
+      for (int m = 0; m < First::PER; ++m) {
+        const int j = t + m * TPL;
+        if (BF % TPL != 0 && j >= BF) continue;
+#pragma unroll
+        for (int r = 0; r < R0; ++r) lay.gload(j + r * BF, vr[m][r], vi[m][r]);
+      }
+    }
+    __syncthreads();  // every thread is done with `stage` (and with `buf`)
+    start(b + gridDim.x, false);
+    First::run(buf, lay, t, a.tw, vr, vi);
+  }
+  if (stale && t == 0) (void)line_wait(bar, stale_parity);
+}
+
+template <typename T, int L, int TPL, int FLAGS, int... Rs>
+__global__ void __launch_bounds__(TPL, (FLAGS & kTwoCtas) ? 2 : 1)
+rows_prefetch_kernel(const RowsArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  rows_prefetch_body<T, L, TPL, FLAGS, Rs...>(a, smem_raw);
 }
 
 // ---------------------------------------------------------------------------

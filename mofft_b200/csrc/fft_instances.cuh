@@ -28,6 +28,8 @@ RowsArgs<T> rows_args(const mofft_pass_args *p) {
   a.sign = p->conj_in ? T(-1) : T(1);
   a.in_table = reinterpret_cast<const cplx_t<T> *const *>(p->in_table);
   a.out_table = reinterpret_cast<cplx_t<T> *const *>(p->out_table);
+  a.status = p->status;
+  a.lose_copy = p->lose_copy;
   return a;
 }
 
@@ -54,17 +56,49 @@ ColsArgs<T> cols_args(const mofft_pass_args *p) {
 
 template <typename T, int L, int TPL, int TB, int FLAGS, int... Rs>
 struct RowsInst {
+  static constexpr bool kPf = (FLAGS & kPrefetch) != 0;
+  static_assert(!kPf || (TB == 1 && (FLAGS & kSplitX) != 0 && (FLAGS & kStaged) == 0),
+                "prefetching kernels run one split-exchange line per CTA step");
   static constexpr size_t smem() {
+    if constexpr (kPf) return prefetch_smem<T, L, TPL>();
     return ((FLAGS & kSplitX) ? 1ull : 2ull) * TB * rows_line<T>(L, TPL, TB) * sizeof(T);
   }
   static const void *func() {
-    if constexpr ((FLAGS & kTwoCtas) != 0)
+    if constexpr (kPf)
+      return reinterpret_cast<const void *>(&rows_prefetch_kernel<T, L, TPL, FLAGS, Rs...>);
+    else if constexpr ((FLAGS & kTwoCtas) != 0)
       return reinterpret_cast<const void *>(&rows_kernel_2cta<T, L, TPL, TB, FLAGS, Rs...>);
     else
       return reinterpret_cast<const void *>(&rows_kernel<T, L, TPL, TB, FLAGS, Rs...>);
   }
+  // Prefetching kernels: resident CTAs per SM times the SM count, cached per
+  // device (0 when the device cannot be queried).
+  static int persistent_grid() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    if (cached[dev] > 0) return cached[dev];
+    int sms = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, rows_prefetch_kernel<T, L, TPL, FLAGS, Rs...>, TPL, smem()) !=
+            cudaSuccess)
+      return 0;
+    if (per_sm < 1) return sms;  // shared-memory attribute not set yet: do not cache
+    cached[dev] = per_sm * sms;
+    return cached[dev];
+  }
   static cudaError_t launch(const mofft_pass_args *p, cudaStream_t s) {
     if (p->conj_in != p->conj_out) return cudaErrorInvalidValue;
+    if constexpr (kPf) {
+      if (p->batch <= 0) return cudaSuccess;
+      const int resident = persistent_grid();
+      if (resident <= 0) return cudaErrorInvalidConfiguration;
+      const long long grid = p->batch < resident ? p->batch : resident;
+      rows_prefetch_kernel<T, L, TPL, FLAGS, Rs...>
+          <<<(unsigned)grid, TPL, smem(), s>>>(rows_args<T>(p));
+      return cudaGetLastError();
+    }
     const long long grid = (p->batch + TB - 1) / TB;
     if (grid <= 0) return cudaSuccess;
     if (grid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
@@ -85,6 +119,7 @@ struct RowsInst {
     e.desc.lines = TB;
     e.desc.threads = TPL * TB;
     e.desc.staged = (FLAGS & kStaged) ? 1 : 0;
+    e.desc.prefetch = kPf ? 1 : 0;
     const int rs[] = {Rs...};
     e.desc.radix_count = (int)sizeof...(Rs);
     for (int i = 0; i < 8; ++i) e.desc.radices[i] = i < (int)sizeof...(Rs) ? rs[i] : 0;
@@ -225,6 +260,12 @@ struct GenericInst {
 #define ROWSD2(T, L, TPL, TB, ...) \
   RowsInst<T, L, TPL, TB, kDerivedTw | kTwoCtas, __VA_ARGS__>::entry( \
       "rows_" #T "_" #L "_t" #TPL "_b" #TB "_sfalse_d2")
+#define ROWSP(T, L, TPL, ...) \
+  RowsInst<T, L, TPL, 1, kDerivedTw | kSplitX | kPrefetch, __VA_ARGS__>::entry( \
+      "rows_" #T "_" #L "_t" #TPL "_b1_sfalse_dxp")
+#define ROWSP2(T, L, TPL, ...) \
+  RowsInst<T, L, TPL, 1, kDerivedTw | kSplitX | kPrefetch | kTwoCtas, __VA_ARGS__>::entry( \
+      "rows_" #T "_" #L "_t" #TPL "_b1_sfalse_dxp2")
 #define COLS(T, L, TPL, C, ...) \
   ColsInst<T, L, TPL, C, __VA_ARGS__>::entry("cols_" #T "_" #L "_t" #TPL "_c" #C)
 

@@ -50,6 +50,12 @@ const Entry *entries_rows_f32(int *count) {
       ROWSX(float, 8192, 512, 1, 16, 16, 16, 2),
       ROWSX(float, 16384, 512, 1, 16, 16, 16, 4),
       ROWSX(float, 16384, 1024, 1, 16, 16, 16, 4),
+      // persistent CTAs, next line bulk-copied while this one is transformed
+      // (measured on 2^26 points against the kernels above: ahead only for
+      // 16384, 0.55 against 0.51 of the HBM roofline; at 4096-12288 and for
+      // FP64 2048-8192 the same scheme measured 0-30 % slower, the lines
+      // being bound by registers and exchanges rather than by load latency)
+      ROWSP(float, 16384, 512, 32, 32, 16),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;

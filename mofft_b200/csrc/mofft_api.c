@@ -600,6 +600,20 @@ static int is_tensor_kind(int kind) {
   return kind == MOFFT_KERNEL_TENSOR || kind == MOFFT_KERNEL_TENSOR_COLS;
 }
 
+/* Passes whose kernel reports bounded-wait timeouts in an error word: the
+ * tensor-core kernels and the prefetching ROWS kernels. */
+static int pass_has_status(const mofft_pass *ps) {
+  if (is_tensor_kind(ps->kind)) return 1;
+  const mofft_kernel_desc *d = mofft_cuda_kernel_get(ps->kernel);
+  return ps->kind == MOFFT_KERNEL_ROWS && d && d->prefetch;
+}
+
+static int schedule_has_status(const mofft_core *c) {
+  for (int p = 0; p < c->sched.pass_count; ++p)
+    if (pass_has_status(&c->sched.pass[p])) return 1;
+  return 0;
+}
+
 /* Build device state (twiddles, workspace) for c->sched. */
 static mofft_status materialise_schedule(mofft_core *c) {
   const size_t cb = mofft_complex_bytes(c->precision_bits);
@@ -625,6 +639,8 @@ static mofft_status materialise_schedule(mofft_core *c) {
     if (is_tensor_kind(ps->kind)) {
       ps->aux_offset = bytes;
       bytes = align256(bytes + mofft_cuda_tensor_aux_bytes(mofft_cuda_kernel_get(ps->kernel)->form));
+    }
+    if (pass_has_status(ps)) {
       ps->status_offset = bytes;
       bytes = align256(bytes + sizeof(int));
     }
@@ -749,12 +765,16 @@ static mofft_status build_tensor_schedule(mofft_core *c) {
   return materialise_schedule(c);
 }
 
-/* Failure check of the tensor-core one-pass kernel: one launch whose first
- * input copy is never issued, so every CTA's bounded wait runs out.  Returns
- * the status the plan then reports (MOFFT_INTERNAL_ERROR when the timeout
- * path works) and clears the error word, so the plan stays usable. */
+/* Failure check of a one-pass plan whose kernel bulk-copies its input (the
+ * tensor-core kernel, a prefetching ROWS kernel): one forward launch whose
+ * first input copy per CTA is never issued, so every CTA's bounded wait runs
+ * out.  Returns the status the plan then reports (MOFFT_INTERNAL_ERROR when
+ * the timeout path works) and clears the error word, so the plan stays
+ * usable.  The ROWS kernel loads the line itself after the timeout, so its
+ * output is still the forward transform. */
 mofft_status mofft_core_check_lost_copy(mofft_core *c, const void *in, void *out) {
-  if (c->sched.pass_count != 1 || c->sched.pass[0].kind != MOFFT_KERNEL_TENSOR)
+  if (c->sched.pass_count != 1 || c->sched.pass[0].kind == MOFFT_KERNEL_TENSOR_COLS ||
+      !pass_has_status(&c->sched.pass[0]))
     return MOFFT_INVALID_ARGUMENT;
   const mofft_pass *ps = &c->sched.pass[0];
   mofft_pass_args a;
@@ -762,7 +782,7 @@ mofft_status mofft_core_check_lost_copy(mofft_core *c, const void *in, void *out
   a.in = in;
   a.out = out;
   a.tw = (const unsigned char *)c->d_twiddles + ps->tw_offset;
-  a.aux = (const unsigned char *)c->d_twiddles + ps->aux_offset;
+  if (is_tensor_kind(ps->kind)) a.aux = (const unsigned char *)c->d_twiddles + ps->aux_offset;
   a.status = (int *)((unsigned char *)c->d_twiddles + ps->status_offset);
   a.batch = (long long)c->batch;
   a.in_dist = (long long)c->distance;
@@ -789,7 +809,7 @@ mofft_status mofft_core_check_lost_copy(mofft_core *c, const void *in, void *out
 mofft_status mofft_core_check_status(const mofft_core *c) {
   for (int p = 0; p < c->sched.pass_count; ++p) {
     const mofft_pass *ps = &c->sched.pass[p];
-    if (!is_tensor_kind(ps->kind)) continue;
+    if (!pass_has_status(ps)) continue;
     int word = 0;
     if (cudaMemcpy(&word, (const unsigned char *)c->d_twiddles + ps->status_offset,
                    sizeof(word), cudaMemcpyDeviceToHost) != cudaSuccess) {
@@ -952,10 +972,10 @@ static mofft_status enqueue_with_work(const mofft_core *c, const void *in, void 
     a.split_shift = ps->split_shift;
     a.conj_in = backward && p == 0;
     a.conj_out = backward && p == P - 1;
-    if (is_tensor_kind(ps->kind)) {
+    if (is_tensor_kind(ps->kind))
       a.aux = (const unsigned char *)c->d_twiddles + ps->aux_offset;
+    if (pass_has_status(ps))
       a.status = (int *)((unsigned char *)c->d_twiddles + ps->status_offset);
-    }
     a.generic_cols = P > 1;
     a.length = ps->length;
     a.lines = ps->lines;
@@ -1023,7 +1043,7 @@ mofft_status mofft_core_execute(const mofft_core *cc, const void *in, void *out)
       cudaGetLastError();
       st = MOFFT_INTERNAL_ERROR;
     }
-    if (st == MOFFT_SUCCESS && !c->user_stream && c->form != 0)
+    if (st == MOFFT_SUCCESS && !c->user_stream && schedule_has_status(c))
       st = mofft_core_check_status(c);
   } else if (dev_in != dev_out) {
     st = MOFFT_INVALID_ARGUMENT; /* mixed host/device buffers */
@@ -1066,7 +1086,7 @@ mofft_status mofft_core_execute(const mofft_core *cc, const void *in, void *out)
         if (cudaStreamSynchronize(streams[i]) != cudaSuccess && st == MOFFT_SUCCESS)
           st = MOFFT_INTERNAL_ERROR;
       if (st != MOFFT_SUCCESS) cudaGetLastError();
-      if (st == MOFFT_SUCCESS && c->form != 0) st = mofft_core_check_status(c);
+      if (st == MOFFT_SUCCESS && schedule_has_status(c)) st = mofft_core_check_status(c);
     }
     pthread_mutex_unlock(&c->lock);
   }
@@ -1157,6 +1177,8 @@ mofft_status mofft_core_enqueue_indirect(const mofft_core *c, const void *const 
     a.lines = ps->lines;
     a.radix_count = ps->radix_count;
     memcpy(a.radices, ps->radices, sizeof(a.radices));
+    if (pass_has_status(ps))
+      a.status = (int *)((unsigned char *)c->d_twiddles + ps->status_offset);
     const int err = mofft_cuda_launch_pass(ps->kernel, &a, stream);
     atomic_fetch_add(&g_launches, 1);
     if (err != 0) {

@@ -37,6 +37,8 @@ typedef struct {
   int radices[8];
   size_t smem_bytes;    /* dynamic shared memory per CTA */
   int form;             /* mofft_precision_form; 0 for the CUDA-core kernels */
+  int prefetch;         /* ROWS: persistent CTAs that bulk-copy the next line
+                           (the pass takes an error word, `status`) */
 } mofft_kernel_desc;
 
 typedef struct {
@@ -58,8 +60,9 @@ typedef struct {
    * kernels only). */
   const void *const *in_table;
   void *const *out_table;
-  /* tensor-core kernels only: constant B operand tiles and the error word
-   * the kernel sets when a wait on the tensor core timed out */
+  /* tensor-core kernels: constant B operand tiles and the error word the
+   * kernel sets when a wait on the tensor core timed out; prefetching ROWS
+   * kernels: the error word their line-copy waits set (may be NULL) */
   const void *aux;
   int *status;
   int lose_copy;         /* failure check: the kernel's first copy is never

@@ -120,6 +120,8 @@ __device__ __forceinline__ RowsArgs<float> rows_args_of(const RItem &it) {  // N
   a.sign = it.sign;
   a.in_table = nullptr;
   a.out_table = nullptr;
+  a.status = nullptr;
+  a.lose_copy = 0;
   return a;
 }
 

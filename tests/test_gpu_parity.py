@@ -263,6 +263,67 @@ def test_every_specialised_kernel():
                 assert rel_l2(y, ref) <= tol, (k["name"], direction, inplace)
 
 
+PREFETCH_KERNEL = "rows_float_16384_t512_b1_sfalse_dxp"
+
+
+def test_prefetching_kernel_many_lines_per_cta():
+    """The persistent kernel that bulk-copies each CTA's next line while it
+    transforms the current one, with more lines than resident CTAs (every CTA
+    runs 2-3 lines), both directions, in and out of place.  With an odd
+    distance every other line start is not 16-byte aligned: those lines are
+    loaded directly and the copies of the aligned ones still pair with their
+    waits."""
+    import torch
+    k = next(k for k in m.kernels() if k["name"] == PREFETCH_KERNEL)
+    n, batch = k["length"], 300
+    for dist in (n, n + 1):
+        buf = oracle.uniform(batch * dist, seed=dist, dtype=np.complex64)
+        x = torch.from_numpy(buf).cuda()
+        lines = buf.reshape(batch, dist)[:, :n].astype(np.complex128)
+        for direction in (-1, 1):
+            ref = oracle_ref(lines, direction)
+            for inplace in (False, True):
+                with m.Plan.create(n, direction, m.IN_PLACE if inplace else m.OUT_OF_PLACE,
+                                   bits=32, batch=batch, distance=dist,
+                                   kernels=[k["index"]]) as plan:
+                    y = x.clone() if inplace else torch.zeros_like(x)
+                    plan.execute(y if inplace else x, y)
+                    plan.check_status()
+                out = y.cpu().numpy().reshape(batch, dist)
+                assert rel_l2(out[:, :n], ref) <= fp32_tol(n), (dist, direction, inplace)
+                if dist > n and not inplace:
+                    assert np.all(out[:, n:] == 0)      # gaps untouched
+
+
+def test_prefetching_kernel_lost_copy_keeps_output():
+    """Failure check of the prefetching kernel: no CTA's first line copy is
+    issued, so every bounded wait runs out (about a second, no GPU fault).
+    The plan reports MOFFT_INTERNAL_ERROR once, the CTAs load those lines
+    themselves so the output is still the forward transform, and the plan
+    then executes normally on the same context."""
+    import time
+    import torch
+    lib = m.load()
+    k = next(k for k in m.kernels() if k["name"] == PREFETCH_KERNEL)
+    n, batch = k["length"], 300
+    x = oracle.uniform(batch * n, seed=12, dtype=np.complex64).reshape(batch, n)
+    ref = oracle_ref(x.astype(np.complex128), -1)
+    d = torch.from_numpy(x).cuda()
+    out = torch.zeros_like(d)
+    with m.Plan.create(n, m.FORWARD, m.OUT_OF_PLACE, bits=32, batch=batch,
+                       kernels=[k["index"]]) as plan:
+        t0 = time.perf_counter()
+        st = lib.mofft_plan_check_lost_copy_f32(plan.handle, d.data_ptr(), out.data_ptr())
+        waited = time.perf_counter() - t0
+        assert st == m.Status.INTERNAL_ERROR
+        assert waited < 30.0, waited
+        assert rel_l2(out.cpu().numpy(), ref) <= fp32_tol(n)
+        plan.check_status()                       # the error word was cleared
+        out.zero_()
+        plan.execute(d, out)
+    assert rel_l2(out.cpu().numpy(), ref) <= fp32_tol(n)
+
+
 def test_batch_distance_and_stream():
     """distance > length leaves the gaps untouched; an attached stream makes
     execute asynchronous on that stream."""
