@@ -301,15 +301,23 @@ def run_reference(args, world, rank):
     return 0
 
 
+L2_BYTES = 126 * 1000 * 1000
+
+
 def workload_config(args) -> dict:
     n = args.n
     batch = max(1, args.points // n)
+    points = batch * n
+    held = points * (8 if args.bits == 32 else 16) * (2 if args.out_of_place else 1)
+    size = f"2^{points.bit_length() - 1}" if points & (points - 1) == 0 else str(points)
+    relation = "> L2 (no flush)" if held > L2_BYTES else "<= L2 (L2-resident: not a HBM figure)"
     return {"workload": f"C2C {'forward' if args.direction < 0 else 'backward'} "
                         f"FP{args.bits} n={n} batch={batch} "
                         f"{'out-of-place' if args.out_of_place else 'in-place'}",
             "n": n, "batch": batch, "precision_bits": args.bits,
             "placement": "out-of-place" if args.out_of_place else "in-place",
-            "inputs": "uniform[-1,1) seeded; 2^26-point working set > L2 (no flush)",
+            "inputs": f"uniform[-1,1) seeded; {size}-point working set of "
+                      f"{held / 1e6:.0f} MB {relation}",
             "parallelism": f"replicas x{args.gpus}", "form": args.form}
 
 

@@ -225,7 +225,7 @@ struct ColsLayout {
 
 // Kernel flags (template parameter FLAGS of the ROWS kernels).
 constexpr int kStaged = 1;       // I/O staged through shared memory
-constexpr int kDerivedTw = 2;    // radix-16 twiddles from w, w^2, w^4, w^8
+constexpr int kDerivedTw = 2;    // radix-16/32 twiddles from w, w^2, w^4, w^8 (, w^16)
 constexpr int kSplitX = 4;       // exchanges move one component at a time
 constexpr int kTwoCtas = 8;      // registers capped for two resident CTAs per SM
 constexpr int kPrefetch = 16;    // persistent CTAs; the next line arrives by bulk copy
@@ -256,6 +256,40 @@ __device__ __forceinline__ void twiddle16_derived(T (&vr)[16], T (&vi)[16], int 
   for (int r = 1; r < 16; ++r) cmul<T>(vr[r], vi[r], wr[r], wi[r]);
 }
 
+// Twiddles of one radix-32 butterfly: w^1 .. w^15 as in the radix-16 case
+// plus the table entry of w^16, and w^(16+k) = w^16 w^k (at most four chained
+// products), so 5 table loads instead of 31.
+template <typename T, int NS, int TWOFF>
+__device__ __forceinline__ void twiddle32_derived(T (&vr)[32], T (&vi)[32], int jm,
+                                                  const cplx_t<T>* __restrict__ tw) {
+  T wr[16], wi[16];
+  const cplx_t<T> a1 = __ldg(tw + TWOFF + 0 * NS + jm);
+  const cplx_t<T> a2 = __ldg(tw + TWOFF + 1 * NS + jm);
+  const cplx_t<T> a4 = __ldg(tw + TWOFF + 3 * NS + jm);
+  const cplx_t<T> a8 = __ldg(tw + TWOFF + 7 * NS + jm);
+  const cplx_t<T> a16 = __ldg(tw + TWOFF + 15 * NS + jm);
+  wr[1] = a1.x; wi[1] = a1.y;
+  wr[2] = a2.x; wi[2] = a2.y;
+  wr[4] = a4.x; wi[4] = a4.y;
+  wr[8] = a8.x; wi[8] = a8.y;
+#define MOFFT_WMUL(D, A, B)                          \
+  wr[D] = wr[A] * wr[B] - wi[A] * wi[B];             \
+  wi[D] = wr[A] * wi[B] + wi[A] * wr[B];
+  MOFFT_WMUL(3, 2, 1) MOFFT_WMUL(5, 4, 1) MOFFT_WMUL(6, 4, 2) MOFFT_WMUL(7, 4, 3)
+  MOFFT_WMUL(9, 8, 1) MOFFT_WMUL(10, 8, 2) MOFFT_WMUL(11, 8, 3) MOFFT_WMUL(12, 8, 4)
+  MOFFT_WMUL(13, 8, 5) MOFFT_WMUL(14, 8, 6) MOFFT_WMUL(15, 8, 7)
+#undef MOFFT_WMUL
+#pragma unroll
+  for (int r = 1; r < 16; ++r) cmul<T>(vr[r], vi[r], wr[r], wi[r]);
+  cmul<T>(vr[16], vi[16], a16.x, a16.y);
+#pragma unroll
+  for (int k = 1; k < 16; ++k) {
+    const T pr = a16.x * wr[k] - a16.y * wi[k];
+    const T pi = a16.x * wi[k] + a16.y * wr[k];
+    cmul<T>(vr[16 + k], vi[16 + k], pr, pi);
+  }
+}
+
 template <typename T, int L, int TPL, int R, int NS, Where SRC, Where DST,
           int TWOFF, bool DTW, class Layout>
 __device__ __forceinline__ void reg_stage(const Layout& lay, int t,
@@ -284,6 +318,8 @@ __device__ __forceinline__ void reg_stage(const Layout& lay, int t,
         const int jm = j % NS;
         if constexpr (DTW && R == 16) {
           twiddle16_derived<T, NS, TWOFF>(vr[m], vi[m], jm, tw);
+        } else if constexpr (DTW && R == 32) {
+          twiddle32_derived<T, NS, TWOFF>(vr[m], vi[m], jm, tw);
         } else {
 #pragma unroll
           for (int r = 1; r < R; ++r) {
@@ -377,6 +413,8 @@ __device__ __forceinline__ void split_compute(T (&vr)[PER][R], T (&vi)[PER][R], 
       const int jm = j % NS;
       if constexpr (DTW && R == 16) {
         twiddle16_derived<T, NS, TWOFF>(vr[m], vi[m], jm, tw);
+      } else if constexpr (DTW && R == 32) {
+        twiddle32_derived<T, NS, TWOFF>(vr[m], vi[m], jm, tw);
       } else {
 #pragma unroll
         for (int r = 1; r < R; ++r) {
@@ -872,7 +910,7 @@ __device__ __forceinline__ void cols_body(const ColsArgs<T>& a, long long b,
   if (a.ns_outer == 1) {
     ColsLayout<T, C, G::PITCH, false> lay;
     cols_layout<T, L, TPL, C, false>(lay, a, b, j0, sre, sim);
-    StageRunner<T, L, TPL, 1, 0, false, true, true, false, Rs...>::run(lay, t, a.tw);
+    StageRunner<T, L, TPL, 1, 0, false, true, true, true, Rs...>::run(lay, t, a.tw);
     // lines j0..j0+C-1 are contiguous: out[b*dist + j0*L + c*L + k]
     cplx_t<T>* dst = batch_out<T>(a.out, a.out_dist, a.out_table, b) + j0 * L;
     if (lay.active) {
@@ -886,7 +924,7 @@ __device__ __forceinline__ void cols_body(const ColsArgs<T>& a, long long b,
   } else {
     ColsLayout<T, C, G::PITCH, true> lay;
     cols_layout<T, L, TPL, C, true>(lay, a, b, j0, sre, sim);
-    StageRunner<T, L, TPL, 1, 0, false, false, true, false, Rs...>::run(lay, t, a.tw);
+    StageRunner<T, L, TPL, 1, 0, false, false, true, true, Rs...>::run(lay, t, a.tw);
   }
 }
 
