@@ -53,6 +53,19 @@ const Entry *entries_rows_mixed(int *count) {
       ROWSX(float, 6144, 384, 1, 6, 4, 16, 16),
       ROWSX(float, 10240, 640, 1, 5, 8, 16, 16),
       ROWSX(float, 12288, 768, 1, 3, 16, 16, 16),
+      // derived radix-16 twiddles (5 table loads per butterfly instead of 15)
+      ROWSD(float, 1280, 80, 2, false, 5, 16, 16),
+      ROWSD(float, 1536, 96, 2, false, 6, 16, 16),
+      ROWSD(float, 2560, 160, 1, false, 10, 16, 16),
+      ROWSD(float, 3072, 192, 1, false, 12, 16, 16),
+      ROWSD(float, 5120, 320, 1, false, 5, 4, 16, 16),
+      ROWSD(float, 6144, 384, 1, false, 6, 4, 16, 16),
+      ROWSD(float, 10240, 640, 1, false, 5, 8, 16, 16),
+      ROWSD(float, 12288, 768, 1, false, 3, 16, 16, 16),
+      ROWSD(double, 1280, 80, 2, false, 5, 16, 16),
+      ROWSD(double, 1536, 96, 2, false, 6, 16, 16),
+      ROWSD(double, 10240, 640, 1, false, 5, 8, 16, 16),
+      ROWSD(double, 12288, 768, 1, false, 3, 16, 16, 16),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;
