@@ -38,8 +38,12 @@ const Entry *entries_rows_mixed(int *count) {
       ROWS(double, 3072, 192, 1, false, 12, 16, 16),
       ROWS(double, 5120, 320, 1, false, 5, 4, 16, 16),
       ROWS(double, 6144, 384, 1, false, 6, 4, 16, 16),
-      ROWS(double, 10240, 640, 1, false, 5, 8, 16, 16),
-      ROWS(double, 12288, 768, 1, false, 3, 16, 16, 16),
+      // derived radix-16 twiddles; registered before the table-twiddle
+      // instances below because the planner takes the first instance of a
+      // chain when no tuned kernel applies (in-place plans, where the tuned
+      // two-pass schedules of these lengths would need a workspace)
+      ROWSD(double, 10240, 640, 1, false, 5, 8, 16, 16),
+      ROWSD(double, 12288, 768, 1, false, 3, 16, 16, 16),
       // split exchanges (one component per exchange: half the shared memory)
       ROWSX(double, 2560, 160, 1, 10, 16, 16),
       ROWSX(double, 3072, 192, 1, 12, 16, 16),
@@ -64,8 +68,8 @@ const Entry *entries_rows_mixed(int *count) {
       ROWSD(float, 12288, 768, 1, false, 3, 16, 16, 16),
       ROWSD(double, 1280, 80, 2, false, 5, 16, 16),
       ROWSD(double, 1536, 96, 2, false, 6, 16, 16),
-      ROWSD(double, 10240, 640, 1, false, 5, 8, 16, 16),
-      ROWSD(double, 12288, 768, 1, false, 3, 16, 16, 16),
+      ROWS(double, 10240, 640, 1, false, 5, 8, 16, 16),
+      ROWS(double, 12288, 768, 1, false, 3, 16, 16, 16),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;
