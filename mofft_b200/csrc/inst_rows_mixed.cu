@@ -58,6 +58,22 @@ const Entry *entries_rows_mixed(int *count) {
       ROWSX(float, 10240, 640, 1, 5, 8, 16, 16),
       ROWSX(float, 12288, 768, 1, 3, 16, 16, 16),
       // derived radix-16 twiddles (5 table loads per butterfly instead of 15)
+      ROWSD(float, 80, 5, 48, true, 5, 16),
+      ROWSD(float, 96, 6, 32, true, 6, 16),
+      ROWSD(float, 160, 10, 24, true, 10, 16),
+      ROWSD(float, 192, 12, 16, true, 12, 16),
+      ROWSD(float, 320, 20, 8, true, 5, 4, 16),
+      ROWSD(float, 384, 24, 8, true, 6, 4, 16),
+      ROWSD(float, 640, 40, 4, false, 5, 8, 16),
+      ROWSD(float, 768, 48, 4, false, 3, 16, 16),
+      ROWSD(double, 80, 5, 24, true, 5, 16),
+      ROWSD(double, 96, 6, 16, true, 6, 16),
+      ROWSD(double, 160, 10, 12, true, 10, 16),
+      ROWSD(double, 192, 12, 8, true, 12, 16),
+      ROWSD(double, 320, 20, 4, true, 5, 4, 16),
+      ROWSD(double, 384, 24, 4, true, 6, 4, 16),
+      ROWSD(double, 640, 40, 4, false, 5, 8, 16),
+      ROWSD(double, 768, 48, 4, false, 3, 16, 16),
       ROWSD(float, 1280, 80, 2, false, 5, 16, 16),
       ROWSD(float, 1536, 96, 2, false, 6, 16, 16),
       ROWSD(float, 2560, 160, 1, false, 10, 16, 16),
