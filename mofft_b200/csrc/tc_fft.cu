@@ -55,8 +55,6 @@ constexpr int kN = 4096;
 constexpr int kR = 16;
 constexpr int kBF = kN / kR;              // 256 butterflies per stage
 constexpr int kThreads = 256;
-constexpr unsigned kMaxWaitIters = 1u << 26;
-constexpr uint64_t kWaitNs = 1000000000ull;  // one second
 
 template <int FORM> struct FormTraits;
 template <> struct FormTraits<kFormTf32x3> {
@@ -205,44 +203,9 @@ __device__ __forceinline__ void store_split<kFormBf16x3>(uint32_t a_hi, uint32_t
   tmem_st16(a_lo, l);
 }
 
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Bounded wait for the completion of the mbarrier phase of `parity`: gives up
-// after kWaitNs of wall time (or kMaxWaitIters polls) and returns false.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  const uint64_t t0 = global_ns();
-  for (unsigned it = 0; it < kMaxWaitIters; ++it) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if ((it & 63u) == 63u && global_ns() - t0 > kWaitNs) return false;
-  }
-  return false;
-}
-
-// One transform's 32 KB into shared memory by a bulk asynchronous copy that
-// completes a transaction count on `bar` (no multicast).
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes,
-                                          uint32_t bar) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-               "r"(bytes)
-               : "memory");
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
-      "[%3];" ::"r"(dst),
-      "l"(src), "r"(bytes), "r"(bar)
-      : "memory");
-}
+// Waits and copies: line_wait (bounded mbarrier wait, one second of
+// %globaltimer) and line_copy (one bulk asynchronous copy of a transform's
+// 32 KB, no multicast) of fft_device.cuh.
 
 template <int FORM>
 __device__ __forceinline__ void issue_mmas(uint32_t tmem, uint32_t b_hi, uint32_t b_lo) {
@@ -371,7 +334,7 @@ __global__ void __launch_bounds__(kThreads, FormTraits<FORM>::kMinBlocks)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
   if (a.bulk && !a.lose_copy && tid == 0 && (long long)blockIdx.x < a.batch)
-    bulk_load(in_addr, a.in + (long long)blockIdx.x * a.in_dist, kN * 8, load_bar);
+    line_copy(in_addr, a.in + (long long)blockIdx.x * a.in_dist, kN * 8, load_bar);
 
   const int j = tid;        // this thread's butterfly = its row of A and D
   const int tile = j >> 7;  // M tile; the TMEM lane is j & 127 = 32 (warp & 3) + lane
@@ -392,7 +355,7 @@ __global__ void __launch_bounds__(kThreads, FormTraits<FORM>::kMinBlocks)
     const float2 *gin = a.in + b * a.in_dist;
     float2 *gout = a.out + b * a.out_dist;
     if (a.bulk) {
-      const bool ok = mbar_wait(load_bar, load_phase);
+      const bool ok = line_wait(load_bar, load_phase);
       if (__syncthreads_or(!ok)) {
         failed = true;
         break;
@@ -436,13 +399,12 @@ __global__ void __launch_bounds__(kThreads, FormTraits<FORM>::kMinBlocks)
             : "memory");
         if (stage == 0 && a.bulk && b + gridDim.x < a.batch) {
           // every thread has read this transform's input: prefetch the next
-          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          bulk_load(in_addr, a.in + (b + gridDim.x) * a.in_dist, kN * 8, load_bar);
+          line_copy(in_addr, a.in + (b + gridDim.x) * a.in_dist, kN * 8, load_bar);
           load_pending = 1;
         }
       }
       mma_pending = 1;
-      const bool ok = mbar_wait(mma_bar, mma_phase);
+      const bool ok = line_wait(mma_bar, mma_phase);
       if (__syncthreads_or(!ok)) {
         failed = true;
         break;
@@ -480,8 +442,8 @@ __global__ void __launch_bounds__(kThreads, FormTraits<FORM>::kMinBlocks)
       atomicExch(a.status, 1);
       // bounded waits for this CTA's own work in flight before its shared
       // memory and TMEM are released
-      if (mma_pending) (void)mbar_wait(mma_bar, mma_phase);
-      if (load_pending) (void)mbar_wait(load_bar, load_phase);
+      if (mma_pending) (void)line_wait(mma_bar, mma_phase);
+      if (load_pending) (void)line_wait(load_bar, load_phase);
     }
   }
   __syncthreads();
@@ -728,7 +690,7 @@ __global__ void __launch_bounds__(kThreads, FormTraits<FORM>::kMinBlocks)
             : "memory");
       }
       mma_pending = 1;
-      const bool ok = mbar_wait(mma_bar, mma_phase);
+      const bool ok = line_wait(mma_bar, mma_phase);
       if (__syncthreads_or(!ok)) {
         failed = true;
         break;
@@ -780,7 +742,7 @@ __global__ void __launch_bounds__(kThreads, FormTraits<FORM>::kMinBlocks)
   }
   if (failed && tid == 0) {
     atomicExch(a.status, 1);
-    if (mma_pending) (void)mbar_wait(mma_bar, mma_phase);
+    if (mma_pending) (void)line_wait(mma_bar, mma_phase);
   }
   __syncthreads();
   if (warp == 0) {
