@@ -237,6 +237,44 @@ def test_tensor_forms_registered_and_never_planned():
     assert all(ks[k]["kind"] == m.KERNEL_COLS for k in s["kernels"])
 
 
+def test_wisdom_names_compiled_kernels():
+    """Every kernel instance the committed wisdom names is in the compiled
+    registry with that entry's precision, and the named kernels multiply out
+    to the entry's length with its radix chain (a tuned schedule that names a
+    removed or renamed instance would silently fall back to the model)."""
+    import json
+    from pathlib import Path
+    wisdom = json.loads((Path(m.__file__).parent / "wisdom" / "b200_wisdom.json").read_text())
+    ks = {k["name"]: k for k in m.kernels()}
+    for e in wisdom["entries"]:
+        assert int(np.prod(e["chain"])) == e["length"], e
+        if e["kernel_bank"] != 0:
+            continue
+        assert e["kernels"], e
+        total = 1
+        for name in e["kernels"]:
+            assert name in ks, (e["length"], e["precision_bits"], name)
+            assert ks[name]["precision_bits"] == e["precision_bits"], name
+            total *= ks[name]["length"]
+        assert total == e["length"], e
+
+
+def test_prefetching_kernel_registered():
+    """The persistent prefetching one-pass kernel: one line per CTA step,
+    512 threads, chain (32, 32, 16) for FP32 16384, and the compiled wisdom
+    selects it for that length."""
+    import json
+    from pathlib import Path
+    ks = [k for k in m.kernels() if k["name"] == "rows_float_16384_t512_b1_sfalse_dxp"]
+    assert len(ks) == 1
+    k = ks[0]
+    assert (k["kind"], k["precision_bits"], k["length"], k["lines"], k["threads"],
+            k["radices"]) == (m.KERNEL_ROWS, 32, 16384, 1, 512, [32, 32, 16])
+    wisdom = json.loads((Path(m.__file__).parent / "wisdom" / "b200_wisdom.json").read_text())
+    e = [e for e in wisdom["entries"] if e["length"] == 16384 and e["precision_bits"] == 32]
+    assert e and e[0]["kernels"] == [k["name"]]
+
+
 def test_mixed_lengths_use_specialised_kernels():
     """3*2^k and 5*2^k lengths of the plain-method sweep run on specialised
     kernels (no runtime-stage kernel), single pass up to 12288 / 10240."""
