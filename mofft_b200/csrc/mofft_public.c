@@ -7,12 +7,12 @@
  * observe the same contract.  The work itself is delegated to the GPU core
  * (mofft_api.c). */
 #include <cuda_runtime_api.h>
-#include <errno.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
 #include "mofft_host.h"
+#include "mofft_recipe.h"
 
 #ifndef MOFFT_BINARY_ID
 #define MOFFT_BINARY_ID "0000000000000000000000000000000000000000000000000000000000000000"
@@ -22,7 +22,6 @@
 #define DEFAULT_TIMING_SAMPLES 5
 #define MAX_SEARCH_CANDIDATES 64
 #define MAX_TIMING_SAMPLES 31
-#define RECIPE_MAX_BYTES 1024
 
 /* ------------------------------------------------------------------------ */
 /* options and diagnostics                                                   */
@@ -305,163 +304,12 @@ mofft_status mofft_plan_check_f32(mofft_plan_f32 *plan) {
 
 const char *mofft_build_id(void) { return MOFFT_BINARY_ID; }
 
-static int recipe_id_is_valid(const char *id) {
-  if (!id || strlen(id) != 64) return 0;
-  for (size_t i = 0; i < 64; ++i)
-    if (!((id[i] >= '0' && id[i] <= '9') || (id[i] >= 'a' && id[i] <= 'f')))
-      return 0;
-  return 1;
-}
-
-static int parse_uint_token(const char *token, int base, uint64_t *value) {
-  if (!token || !*token || !value) return 0;
-  for (const char *p = token; *p; ++p) {
-    const int digit = *p >= '0' && *p <= '9';
-    const int hex = base == 16 && ((*p >= 'a' && *p <= 'f') || (*p >= 'A' && *p <= 'F'));
-    if (!digit && !hex) return 0;
-  }
-  errno = 0;
-  char *end = NULL;
-  const unsigned long long parsed = strtoull(token, &end, base);
-  if (errno == ERANGE || !end || *end != '\0') return 0;
-  *value = (uint64_t)parsed;
-  return 1;
-}
-
-/* Split on single spaces; a doubled space is malformed (returns SIZE_MAX). */
-static size_t split_tokens(char *text, char **tokens, size_t capacity) {
-  size_t count = 0;
-  char *cursor = text;
-  while (*cursor) {
-    if (count == capacity) return SIZE_MAX;
-    tokens[count++] = cursor;
-    while (*cursor && *cursor != ' ') ++cursor;
-    if (*cursor == ' ') {
-      *cursor++ = '\0';
-      if (*cursor == ' ') return SIZE_MAX;
-    }
-  }
-  return count;
-}
-
-typedef struct {
-  uint32_t family;
-  size_t length;
-  mofft_direction direction;
-  mofft_placement placement;
-  unsigned bank;
-  uint64_t mask;
-  int direct_input;
-  mofft_stage_layout layout;
-  size_t depth;
-  int radices[MOFFT_MAX_STAGES];
-} recipe_fields;
-
-static mofft_status parse_recipe(const char *recipe, size_t size,
-                                 int precision_bits, recipe_fields *f) {
-  if (!recipe || size < 2 || size > RECIPE_MAX_BYTES || recipe[size - 1] != '\0' ||
-      recipe[size - 2] != '\n' || memchr(recipe, '\0', size - 1) != NULL)
-    return MOFFT_INVALID_ARGUMENT;
-  char text[RECIPE_MAX_BYTES];
-  for (size_t i = 0; i < size - 2; ++i) {
-    const unsigned char ch = (unsigned char)recipe[i];
-    if (ch < 32 || ch > 126) return MOFFT_INVALID_ARGUMENT;
-    text[i] = (char)ch;
-  }
-  text[size - 2] = '\0';
-  if (size > 3 && text[size - 3] == ' ') return MOFFT_INVALID_ARGUMENT;
-  char *tokens[12 + MOFFT_MAX_STAGES];
-  const size_t n = split_tokens(text, tokens, 12 + MOFFT_MAX_STAGES);
-  if (n == SIZE_MAX || n < 13 || strcmp(tokens[0], "MOFFT_PLAN_V1") != 0 ||
-      !recipe_id_is_valid(MOFFT_BINARY_ID) || strlen(tokens[1]) != 64 ||
-      strcmp(tokens[1], MOFFT_BINARY_ID) != 0)
-    return MOFFT_INCOMPATIBLE_RECIPE;
-  if (strlen(tokens[2]) != 8 || strlen(tokens[8]) != 16) return MOFFT_INVALID_ARGUMENT;
-  uint64_t family = 0, length = 0, placement = 0, bank = 0, mask = 0;
-  uint64_t direct = 0, layout = 0, depth = 0;
-  if (!parse_uint_token(tokens[2], 16, &family) || family > UINT32_MAX ||
-      !parse_uint_token(tokens[4], 10, &length) ||
-      !parse_uint_token(tokens[6], 10, &placement) ||
-      !parse_uint_token(tokens[7], 10, &bank) ||
-      !parse_uint_token(tokens[8], 16, &mask) ||
-      !parse_uint_token(tokens[9], 10, &direct) ||
-      !parse_uint_token(tokens[10], 10, &layout) ||
-      !parse_uint_token(tokens[11], 10, &depth))
-    return MOFFT_INVALID_ARGUMENT;
-  if ((precision_bits == 32 && strcmp(tokens[3], "f32") != 0) ||
-      (precision_bits == 64 && strcmp(tokens[3], "f64") != 0))
-    return MOFFT_INCOMPATIBLE_RECIPE;
-  if ((strcmp(tokens[5], "-1") != 0 && strcmp(tokens[5], "1") != 0) ||
-      (uint64_t)(size_t)length != length || length < 2 ||
-      placement > MOFFT_IN_PLACE || bank >= MOFFT_KERNEL_BANK_COUNT ||
-      direct > 1 || layout > MOFFT_STAGE_LAYOUT_SECTION || depth == 0 ||
-      depth > MOFFT_MAX_STAGES || n != 12 + (size_t)depth)
-    return MOFFT_INVALID_ARGUMENT;
-  if ((size_t)depth - 1 < 64 && (mask >> ((size_t)depth - 1)) != 0)
-    return MOFFT_INVALID_ARGUMENT;
-  f->family = (uint32_t)family;
-  f->length = (size_t)length;
-  f->direction = strcmp(tokens[5], "-1") == 0 ? MOFFT_FORWARD : MOFFT_BACKWARD;
-  f->placement = (mofft_placement)placement;
-  f->bank = (unsigned)bank;
-  f->mask = mask;
-  f->direct_input = (int)direct;
-  f->layout = (mofft_stage_layout)layout;
-  f->depth = (size_t)depth;
-  size_t remaining = f->length;
-  for (size_t i = 0; i < f->depth; ++i) {
-    uint64_t radix = 0;
-    if (!parse_uint_token(tokens[12 + i], 10, &radix) || radix > INT32_MAX ||
-        radix < 2 || remaining % (size_t)radix != 0)
-      return MOFFT_INVALID_ARGUMENT;
-    f->radices[i] = (int)radix;
-    remaining /= (size_t)radix;
-  }
-  if (remaining != 1) return MOFFT_INVALID_ARGUMENT;
-  uint32_t current = 0;
-  if (!mofft_device_family(&current) || current != f->family)
-    return MOFFT_INCOMPATIBLE_RECIPE;
-  if (!mofft_hardware_supports(precision_bits)) return MOFFT_UNSUPPORTED_HARDWARE;
-  return MOFFT_SUCCESS;
-}
-
-static mofft_status export_core(const mofft_core *c, char *buffer,
-                                size_t capacity, size_t *required) {
-  if (!c || !required) return MOFFT_INVALID_ARGUMENT;
-  uint32_t family = 0;
-  if (!mofft_device_family(&family) || !recipe_id_is_valid(MOFFT_BINARY_ID))
-    return MOFFT_UNSUPPORTED_HARDWARE;
-  char recipe[RECIPE_MAX_BYTES];
-  int written = snprintf(recipe, sizeof(recipe),
-                         "MOFFT_PLAN_V1 %s %08x f%d %zu %d %d %u %016llx %d %d %d",
-                         MOFFT_BINARY_ID, family, c->precision_bits, c->length,
-                         c->direction, (int)c->placement, c->kernel_bank,
-                         (unsigned long long)c->blocked_transpose_mask,
-                         c->direct_input, (int)c->stage_layout, c->depth);
-  if (written < 0 || (size_t)written >= sizeof(recipe)) return MOFFT_INTERNAL_ERROR;
-  size_t used = (size_t)written;
-  for (int i = 0; i < c->depth; ++i) {
-    written = snprintf(recipe + used, sizeof(recipe) - used, " %d", c->factors[i]);
-    if (written < 0 || (size_t)written >= sizeof(recipe) - used)
-      return MOFFT_INTERNAL_ERROR;
-    used += (size_t)written;
-  }
-  if (used + 2 > sizeof(recipe)) return MOFFT_INTERNAL_ERROR;
-  recipe[used++] = '\n';
-  recipe[used] = '\0';
-  *required = used + 1;
-  if (!buffer) return capacity == 0 ? MOFFT_SUCCESS : MOFFT_INVALID_ARGUMENT;
-  if (capacity < *required) return MOFFT_BUFFER_TOO_SMALL;
-  memcpy(buffer, recipe, *required);
-  return MOFFT_SUCCESS;
-}
-
 static mofft_status import_core(mofft_core **out, int precision_bits,
                                 const char *recipe, size_t size,
                                 mofft_plan_diagnostics *diagnostics) {
   if (diagnostics) memset(diagnostics, 0, sizeof(*diagnostics));
-  recipe_fields f;
-  mofft_status st = parse_recipe(recipe, size, precision_bits, &f);
+  mofft_recipe f;
+  mofft_status st = mofft_recipe_read(recipe, size, precision_bits, &f);
   if (st != MOFFT_SUCCESS) return st;
   st = create_with_radices(out, precision_bits, f.length, 1, 0, f.direction,
                            f.placement, f.radices, f.depth);
@@ -663,7 +511,8 @@ static mofft_status create_with_kernels(mofft_core **out, int precision_bits,
   }                                                                              \
   mofft_status mofft_plan_export_##SUF(const PLAN *plan, char *buffer,           \
                                        size_t capacity, size_t *required) {      \
-    return export_core(plan ? CORE(plan) : NULL, buffer, capacity, required);    \
+    return mofft_recipe_write(plan ? CORE(plan) : NULL, buffer, capacity,       \
+                              required);                                         \
   }                                                                              \
   mofft_status mofft_plan_import_##SUF(PLAN **out, const char *recipe,           \
                                        size_t recipe_size,                       \

@@ -126,13 +126,62 @@ def test_recipe_rejections_without_device():
         trailing = raw + b"x\0"
         assert f(ctypes.byref(h), trailing, len(trailing), None) == m.Status.INVALID_ARGUMENT
         spaced = good.replace(" 4 4 4", "  4 4 4").encode() + b"\0"
-        assert f(ctypes.byref(h), spaced, len(spaced), None) == m.Status.INCOMPATIBLE_RECIPE \
-            or True
+        assert f(ctypes.byref(h), spaced, len(spaced), None) == m.Status.INCOMPATIBLE_RECIPE
     # precision mismatch is checked before the device family
     h = ctypes.c_void_p(1)
     raw = good.encode() + b"\0"
     assert lib.mofft_plan_import_f64(ctypes.byref(h), raw, len(raw), None) == \
         m.Status.INCOMPATIBLE_RECIPE
+
+
+def test_recipe_status_per_malformed_field():
+    """One malformed field at a time, and the precedence between kinds of
+    failure, as the reference's recipe parser ranks them
+    (src/mofft.c:1760-1842, tests/test_plan_recipe.c:196-241).  A valid
+    recipe needs the device family, so these cases stop short of it."""
+    lib = m.load()
+    bid = m.build_id()
+    head = f"MOFFT_PLAN_V1 {bid}"
+    INV, INC = m.Status.INVALID_ARGUMENT, m.Status.INCOMPATIBLE_RECIPE
+    cases = [
+        (f"{head} 0a000094 f32 64 -1 0 0 0000000000000000 1 0 3 4 4 4 4", INV),  # depth/count
+        (f"{head} 0a00094 f32 64 -1 0 0 0000000000000000 1 0 3 4 4 4", INV),  # family width
+        (f"{head} 0a00009g f32 64 -1 0 0 0000000000000000 1 0 3 4 4 4", INV),  # family digit
+        (f"{head} 0a000094 f32 64 -1 0 0 000000000000000 1 0 3 4 4 4", INV),  # mask width
+        (f"{head} 0a000094 f32 6x -1 0 0 0000000000000000 1 0 3 4 4 4", INV),  # length digit
+        (f"{head} 0a000094 f32 64 2 0 0 0000000000000000 1 0 3 4 4 4", INV),  # direction
+        (f"{head} 0a000094 f32 64 -1 2 0 0000000000000000 1 0 3 4 4 4", INV),  # placement
+        (f"{head} 0a000094 f32 64 -1 0 2 0000000000000000 1 0 3 4 4 4", INV),  # bank
+        (f"{head} 0a000094 f32 64 -1 0 0 0000000000000004 1 0 3 4 4 4", INV),  # mask bit
+        (f"{head} 0a000094 f32 64 -1 0 0 0000000000000000 2 0 3 4 4 4", INV),  # direct input
+        (f"{head} 0a000094 f32 64 -1 0 0 0000000000000000 1 2 3 4 4 4", INV),  # layout
+        (f"{head} 0a000094 f32 64 -1 0 0 0000000000000000 1 0 0 64", INV),  # depth 0
+        (f"{head} 0a000094 f32 64 -1 0 0 0000000000000000 1 0 3 4 4 5", INV),  # chain
+        (f"{head} 0a000094 f32 64 -1 0 0 0000000000000000 1 0 3 4 4 2", INV),  # product
+        (f"{head} 0a000094 f32 64 -1 0 0 0000000000000000 1 0 3 4 1 16", INV),  # radix 1
+        (f"{head} 0a000094 f32 1 -1 0 0 0000000000000000 1 0 1 1", INV),  # length 1
+        (f"{head} 0a000094 f32 64 -1 0 0 0000000000000000 1 0", INC),  # too few fields
+        (f"{head} 0a000094 f32 64 -1 0 0 0000000000000000 1 0 3 4  4 4", INC),  # blank pair
+        (f"{head} 0a000094 f32 64 -1 0 0 0000000000000000 1 0 3 4 4 4 ", INV),  # trailing blank
+        (f"{head} 0a000094 f32 64 -1 0 0 0000000000000000 1 0 64" + " 2" * 77, INC),  # fields
+        (f"{head} 0a000094 f16 64 -1 0 0 0000000000000000 1 0 3 4 4 4", INC),  # precision
+        # the precision tag outranks value failures, syntax outranks the tag
+        (f"{head} 0a000094 f64 64 -1 0 0 0000000000000000 1 0 3 4 4 x", INC),
+        (f"{head} 0a000094 f64 64 3 0 0 0000000000000000 1 0 3 4 4 4", INC),
+        (f"{head} 0a000094 f64 6x -1 0 0 0000000000000000 1 0 3 4 4 4", INV),
+        # the magic and build id outrank every field check
+        (f"MOFFT_PLAN_V2 {bid} 0a00094 f64 64 -1 0 0 0000000000000000 1 0 3 4 4 4", INC),
+        ("\tMOFFT", INV),  # character set
+    ]
+    for text, expected in cases:
+        raw = text.encode() + b"\n\0"
+        h = ctypes.c_void_p(1)
+        st = lib.mofft_plan_import_f32(ctypes.byref(h), raw, len(raw), None)
+        assert st == expected, (text, st)
+        assert h.value is None
+    big = b"MOFFT_PLAN_V1" + b" 2" * 600 + b"\n\0"  # beyond the 1024-byte limit
+    h = ctypes.c_void_p(1)
+    assert lib.mofft_plan_import_f32(ctypes.byref(h), big, len(big), None) == INV
 
 
 def _arr(values):
