@@ -46,6 +46,7 @@ if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
 FALLBACK_HBM_GBS = 6650.0
+METRIC = "C2C GFLOP/s (5n log2 n) & % HBM roofline vs plain; serve p50/p99 latency"
 
 
 FORMS = {"fp32": 0, "tf32x3": 1, "bf16x3": 2}   # mofft_precision_form
@@ -71,6 +72,10 @@ def parse_args():
     p.add_argument("--ragged", action="store_true",
                    help="ragged batch: 512 mixed FP32 transforms, persistent launch vs per item")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the C1, precision-form and serving figures of the default run")
+    p.add_argument("--serve-requests", type=int, default=20000,
+                   help="requests of the serving figures in the default run")
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--soak", type=float, default=1.0,
@@ -218,16 +223,16 @@ def dist_teardown(world):
 
 # --------------------------------------------------------------- CPU side
 
-def cpu_baseline(n: int, bits: int, direction: int, seconds: float) -> dict:
+def cpu_baseline(n: int, bits: int, direction: int, seconds: float, points: int) -> dict:
     """The reference transform restated in C (oracle/), timed on all host
-    cores over a bounded sample of the workload: the same n, enough
-    transforms for about `seconds` of work."""
+    cores on the workload's whole batch (`points` points of length n), calls
+    repeated for about `seconds` of work."""
     import numpy as np
 
     import oracle
     cores = os.cpu_count() or 1
     dtype = np.complex64 if bits == 32 else np.complex128
-    batch = max(cores, (1 << 22) // n)
+    batch = max(cores, points // n)
     x = oracle.uniform(n * batch, seed=n, dtype=dtype).reshape(batch, n)
     t_warm = time.perf_counter() + 0.25                          # warm-up >= 0.25 s
     while time.perf_counter() < t_warm:
@@ -271,7 +276,7 @@ def run_reference(args, world, rank):
     cores = os.cpu_count() or 1
     n, bits = args.n, args.bits
     dtype = np.complex64 if bits == 32 else np.complex128
-    batch = max(cores, (1 << 20) // n)
+    batch = max(1, args.points // n)          # the whole configured batch
     x = oracle.uniform(n * batch, seed=n, dtype=dtype).reshape(batch, n)
     for _ in range(args.warmup):
         oracle.fft_port(x, args.direction, threads=cores)
@@ -284,16 +289,16 @@ def run_reference(args, world, rank):
     value = flops_per_transform(n) * batch / (ms / 1e3) / 1e9
     cv = statistics.pstdev(times) / statistics.mean(times) if len(times) > 1 else 0.0
     line = {
-        "impl": "reference", "metric": "C2C GFLOP/s (5n log2 n)", "value": round(value, 3),
+        "impl": "reference", "metric": METRIC, "value": round(value, 3),
         "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if bits == 32 else "f64", "data": "synthetic",
         "config": workload_config(args),
         "cpu_baseline": {"value": round(value, 3), "unit": "GFLOP/s", "cores": cores,
                          "kind": "port", "cv": round(cv, 4),
-                         "sample": f"{batch} transforms of n={n} per step (the reference's "
-                                   "SME kernels cannot run on x86; FFTW 3.3.11: unavailable "
-                                   "on this box)"},
+                         "sample": f"the whole workload, {batch} transforms of n={n}, per "
+                                   "step (out of place; the reference's SME kernels cannot "
+                                   "run on x86; FFTW 3.3.11: unavailable on this box)"},
         "e2e": {"value": round(value, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -407,7 +412,7 @@ def run_gpu(args, world, rank, local):
     line = None
     if rank == 0:
         line = {
-            "metric": "C2C GFLOP/s (5n log2 n)", "value": round(value, 2), "unit": "GFLOP/s",
+            "metric": METRIC, "value": round(value, 2), "unit": "GFLOP/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if bits == 32 else "f64", "data": "synthetic",
@@ -417,6 +422,88 @@ def run_gpu(args, world, rank, local):
                          "kernels": [kernels[k] for k in sched["kernels"]]},
         }
     return line
+
+
+def run_c1(m):
+    """C1: n = 1024, batch 4096, out of place, forward then backward on
+    device buffers (uniform[-1,1), seed 0); GFLOP/s of the pair and the
+    round-trip error backward(forward(x)) / n against x."""
+    import torch
+    n, batch, steps = 1024, 4096, 50
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.view_as_complex(torch.rand((batch, n, 2), generator=g, device="cuda") * 2 - 1)
+    y, z = torch.empty_like(x), torch.empty_like(x)
+    stream = torch.cuda.Stream()
+    fwd = m.Plan.create(n, m.FORWARD, m.OUT_OF_PLACE, bits=32, batch=batch)
+    bwd = m.Plan.create(n, m.BACKWARD, m.OUT_OF_PLACE, bits=32, batch=batch)
+    for p in (fwd, bwd):
+        p.set_stream(stream.cuda_stream)
+    for _ in range(3):
+        fwd.execute(x, y)
+        bwd.execute(y, z)
+    stream.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(steps):
+        fwd.execute(x, y)
+        bwd.execute(y, z)
+    e.record(stream)
+    e.synchronize()
+    ms = s.elapsed_time(e) / steps
+    err = float(torch.linalg.vector_norm((z / n - x).to(torch.complex128)) /
+                torch.linalg.vector_norm(x.to(torch.complex128)))
+    fwd.destroy()
+    bwd.destroy()
+    return {"workload": "C2C FP32 n=1024 batch=4096 out-of-place, forward then backward "
+                        "(working set 96 MB: L2-resident, not a HBM figure)",
+            "ms_fwd_bwd": round(ms, 4),
+            "gflops": round(2 * flops_per_transform(n) * batch / (ms / 1e3) / 1e9, 1),
+            "roundtrip_rel_l2": float(f"{err:.3e}")}
+
+
+def run_forms(m):
+    """Precision forms: FP32 C2C forward, out of place, 2^27 points of the
+    precision mix at n = 4096 (batch 32768) and n = 65536 (batch 2048); per
+    form the time of one call (CUDA events), GFLOP/s, the fraction of the
+    HBM roofline, and the relative L2 error on 64 rows spread over the batch
+    against the FP64 transform of the same rows (the library's own FP64
+    plan, parity-tested against the long-double oracle)."""
+    import torch
+
+    from mofft_b200 import workloads
+    peak, kind = measured_peaks()
+    out = {}
+    for n in (4096, 65536):
+        points = 1 << 27
+        batch = points // n
+        x = workloads.precision_mix_device(points, n, seed=11)
+        y = torch.empty_like(x)
+        rows = torch.linspace(0, batch - 1, 64).long().cuda()
+        xr = x[rows].to(torch.complex128).contiguous()
+        ref = torch.empty_like(xr)
+        with m.Plan.create(n, m.FORWARD, m.OUT_OF_PLACE, bits=64, batch=64) as p64:
+            p64.execute(xr, ref)
+        torch.cuda.synchronize()
+        stream = torch.cuda.Stream()
+        per = {}
+        for name, form in FORMS.items():
+            with m.Plan.create(n, m.FORWARD, m.OUT_OF_PLACE, bits=32, batch=batch) as plan:
+                plan.set_precision_form(form)
+                plan.set_stream(stream.cuda_stream)
+                ms, _ = time_device(plan, x, y, 10, 3, stream, 1)
+            err = float(torch.linalg.vector_norm(y[rows].to(torch.complex128) - ref) /
+                        torch.linalg.vector_norm(ref))
+            alg = passes_for(n, 32) * 16 * points
+            per[name] = {"ms": round(ms, 4),
+                         "gflops": round(flops_per_transform(n) * batch / (ms / 1e3) / 1e9, 1),
+                         "hbm_frac": round(alg / (ms / 1e3) / 1e9 / peak, 3),
+                         "rel_l2": float(f"{err:.3e}")}
+        per["fp32_tolerance"] = float(f"{5e-7 * math.log2(n):.2e}")
+        out[f"n={n} batch={batch}"] = per
+        del x, y
+        torch.cuda.empty_cache()
+    out["peak"] = f"{peak} GB/s of {kind}"
+    return out
 
 
 def apply_form(plan, args):
@@ -563,7 +650,7 @@ def run_ragged(args, world, rank, local):
     return line
 
 
-def run_serve(args, world, rank, local):
+def run_serve(args, world, rank, local, requests=None, fracs=(0.5, 0.9), one_shot=True):
     """Serving stream (seeded): n Zipf(1.1) over 2^8..2^20, batch 1..256,
     80 % FP32 / 20 % FP64, device-resident payloads.  The server (continuous
     batching, 4 streams, 40 GiB admission) and serial plain execution (one
@@ -579,7 +666,7 @@ def run_serve(args, world, rank, local):
     import mofft_b200 as m
     from mofft_b200 import workloads
     torch.cuda.set_device(local)
-    reqs = workloads.serving_stream(args.requests, rate_per_s=1.0, seed=11)
+    reqs = workloads.serving_stream(requests or args.requests, rate_per_s=1.0, seed=11)
     maxpts = max(r["n"] * r["batch"] for r in reqs)
     arena_in = {32: torch.view_as_complex(torch.rand((maxpts, 2), device="cuda") * 2 - 1),
                 64: torch.view_as_complex(torch.rand((maxpts, 2), device="cuda",
@@ -682,11 +769,12 @@ def run_serve(args, world, rank, local):
 
     zeros = [0.0] * len(reqs)
     serial_span, serial_lat = run_serial(zeros)
-    one_shot_span, one_shot_lat = run_serial_one_shot()
+    if one_shot:
+        one_shot_span, one_shot_lat = run_serial_one_shot()
     srv_span, srv_lat, stats = run_server(zeros)
     capacity = len(reqs) / serial_span           # serial requests per second
     rates = {}
-    for frac in (0.5, 0.9):
+    for frac in fracs:
         rate = capacity * frac
         rng = np.random.default_rng(5)
         arrivals = list(np.cumsum(rng.exponential(1.0 / rate, size=len(reqs))))
@@ -698,6 +786,22 @@ def run_serve(args, world, rank, local):
         p.destroy()
     sat_server = summary(srv_span, srv_lat)
     sat_serial = summary(serial_span, serial_lat)
+    # the stream's roofline: every request's minimal-pass bytes at the
+    # measured copy bandwidth
+    peak, peak_kind = measured_peaks()
+    floor_s = sum(passes_for(r["n"], r["bits"]) * 2 * (8 if r["bits"] == 32 else 16) *
+                  r["n"] * r["batch"] for r in reqs) / (peak * 1e9)
+    ceiling = {"gflops": round(total_flops / floor_s / 1e9, 1), "ms": round(floor_s * 1e3, 2),
+               "peak": f"{peak} GB/s of {peak_kind}",
+               "server_over_ceiling": round(sat_server["gflops"] * 1e9 * floor_s / total_flops, 3),
+               "serial_over_ceiling": round(sat_serial["gflops"] * 1e9 * floor_s / total_flops,
+                                            3)}
+    saturation = {"server": sat_server, "serial_plain": sat_serial,
+                  "speedup": round(serial_span / srv_span, 2),
+                  "launches": stats["launches"], "requests": len(reqs)}
+    if one_shot:
+        saturation["serial_plan_per_request"] = summary(one_shot_span, one_shot_lat)
+        saturation["speedup_vs_plan_per_request"] = round(one_shot_span / srv_span, 2)
     return {
         "metric": "serve C2C GFLOP/s (5n log2 n), saturation", "value": sat_server["gflops"],
         "unit": "GFLOP/s", "n_gpus": world, "steps": 1, "warmup": 1,
@@ -707,11 +811,7 @@ def run_serve(args, world, rank, local):
                                "20,000-request stream: n Zipf(1.1) over 2^8..2^20, batch 1..256, "
                                "80% FP32 / 20% FP64, device-resident payloads",
                    "server": {"streams": 4, "hbm_budget_gib": 40}},
-        "saturation": {"server": sat_server, "serial_plain": sat_serial,
-                       "speedup": round(serial_span / srv_span, 2),
-                       "serial_plan_per_request": summary(one_shot_span, one_shot_lat),
-                       "speedup_vs_plan_per_request": round(one_shot_span / srv_span, 2),
-                       "launches": stats["launches"], "requests": len(reqs)},
+        "saturation": saturation, "ceiling": ceiling,
         "poisson": rates,
     }
 
@@ -736,9 +836,23 @@ def main():
                 print(json.dumps(line), flush=True)
             return 0
         line = run_gpu(args, world, rank, local)
+        if rank == 0 and world == 1 and not args.no_extras:
+            import mofft_b200 as m
+            count0 = m.launch_count()
+            line["c1"] = run_c1(m)
+            line["forms"] = run_forms(m)
+            serve = run_serve(args, world, rank, local, requests=args.serve_requests,
+                              fracs=(0.9,), one_shot=False)
+            line["serve"] = {"workload": serve["config"]["workload"],
+                             "p50_ms": serve["saturation"]["server"]["p50_ms"],
+                             "p99_ms": serve["saturation"]["server"]["p99_ms"],
+                             "gflops": serve["saturation"]["server"]["gflops"],
+                             "saturation": serve["saturation"], "ceiling": serve["ceiling"],
+                             "poisson": serve["poisson"]}
+            line["extras_gpu_launches"] = int(m.launch_count() - count0)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.n, args.bits, args.direction,
-                                                args.cpu_seconds)
+                                                args.cpu_seconds, args.points)
         if rank == 0:
             print(json.dumps(line), flush=True)
     finally:

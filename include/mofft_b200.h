@@ -141,10 +141,14 @@ void mofft_ragged_plan_destroy(mofft_ragged_plan *plan);
  * device array of MOFFT_FIXED_SCRATCH_POINTS complex values (32 MiB plus 512
  * KiB of twiddles) that every GPU loading the library holds until exit.
  *
+ * It runs the compiled wisdom's tuned schedule of the length when that has
+ * two passes (the kernels an out-of-place PRETUNED plan runs), else the
+ * model's schedule when that has two.
+ *
  * Limits: batch * length <= MOFFT_FIXED_SCRATCH_POINTS, else
  * MOFFT_UNSUPPORTED_SIZE; lengths that run in one pass (they need no scratch)
- * or in three, also MOFFT_UNSUPPORTED_SIZE; host buffers give
- * MOFFT_INVALID_ARGUMENT.  The first call on each device sets up the array's
+ * and lengths with neither a tuned nor a model two-pass schedule, also
+ * MOFFT_UNSUPPORTED_SIZE; host buffers give MOFFT_INVALID_ARGUMENT.  The first call on each device sets up the array's
  * device address (with that device current), so make that first call before
  * any stream capture on that device.  All calls share the array and it keeps
  * the last call's contents; calls whose executions overlap on the GPU race on

@@ -41,7 +41,8 @@ static __device__ __align__(256) float2 g_fixed_scratch[kScratchPoints + kTwiddl
 std::mutex g_setup_mutex;
 void *g_scratch_address[kMaxDevices];
 
-// One twiddle run: count entries W_den^(k*step), k = 0..count-1, at offset.
+// One twiddle run: count entries W_den^(k*step), k = 0..count-1, at offset
+// (den == 0: count zero entries).
 struct FillRegions {
   int count;
   unsigned long long den[kMaxRegions];
@@ -61,6 +62,10 @@ __global__ void fill_twiddle_regions(float2 *base, const FillRegions d,
       ++r;
     }
     if (r >= d.count) continue;
+    if (d.den[r] == 0) {  // the spare entry behind a stage table
+      base[d.offset[r] + (i - start)] = make_float2(0.0f, 0.0f);
+      continue;
+    }
     const unsigned long long k = i - start;
     const unsigned long long e = (k * d.step[r]) % d.den[r];
     double s, c;
@@ -121,15 +126,28 @@ extern "C" mofft_status mofft_execute_fixed_scratch_f32(
   if (!is_device_memory(input) || !is_device_memory(output))
     return MOFFT_INVALID_ARGUMENT;
 
-  // The same schedule a PRETUNED plan of this length uses; only two-pass
-  // schedules need the intermediate array this entry point provides.
+  // Only two-pass schedules need the intermediate array this entry point
+  // provides.  The tuned schedule of the compiled wisdom runs when it has two
+  // passes (the same kernels an out-of-place PRETUNED plan runs); otherwise
+  // the model's schedule runs when it has two (a tuned three-pass schedule
+  // would need a second intermediate array).
   int chain[MOFFT_MAX_STAGES];
-  const int count = mofft_model_chain(32, 0, length, chain, MOFFT_MAX_STAGES);
-  if (count <= 0) return MOFFT_UNSUPPORTED_SIZE;
+  int preferred[MOFFT_MAX_PASSES];
   mofft_schedule sched;
-  if (!mofft_group_chain(32, 0, chain, count, (long long)length, &sched) ||
-      sched.pass_count != 2)
-    return MOFFT_UNSUPPORTED_SIZE;
+  sched.pass_count = 0;
+  const int tuned = mofft_wisdom_lookup(length, 32, chain, MOFFT_MAX_STAGES, preferred);
+  if (tuned > 0 && preferred[0] >= 0 && preferred[1] >= 0 &&
+      (MOFFT_MAX_PASSES < 3 || preferred[2] < 0)) {
+    if (!mofft_group_chain_preferred(32, 0, chain, tuned, (long long)length, preferred,
+                                     &sched))
+      sched.pass_count = 0;
+  }
+  if (sched.pass_count != 2) {
+    const int count = mofft_model_chain(32, 0, length, chain, MOFFT_MAX_STAGES);
+    if (count <= 0 || !mofft_group_chain(32, 0, chain, count, (long long)length, &sched))
+      return MOFFT_UNSUPPORTED_SIZE;
+  }
+  if (sched.pass_count != 2) return MOFFT_UNSUPPORTED_SIZE;
 
   // Twiddle layout: per pass the internal stage table, then (second pass)
   // the two-level super-stage table, as the plan builder lays them out.
@@ -157,6 +175,13 @@ extern "C" mofft_status mofft_execute_fixed_scratch_f32(
       }
       ns *= R;
     }
+    // one spare entry behind the stage table, zero as in a plan's table
+    if (regions.count >= kMaxRegions) return MOFFT_UNSUPPORTED_SIZE;
+    regions.den[regions.count] = 0;
+    regions.step[regions.count] = 0;
+    regions.entries[regions.count] = 1;
+    regions.offset[regions.count] = (unsigned int)cursor;
+    ++regions.count;
     cursor = round32(cursor + 1);
     hi_off[p] = lo_off[p] = cursor;
     if (ps.ns_outer > 1) {

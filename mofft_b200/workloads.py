@@ -63,3 +63,31 @@ def precision_mix(points: int, n: int, seed: int = 3) -> np.ndarray:
     j = np.arange(n)
     out[half:] = np.exp(2j * np.pi * np.outer(bins, j) / n).astype(np.complex64)
     return out
+
+
+def precision_mix_device(points: int, n: int, seed: int = 3, device: str = "cuda"):
+    """The precision mix generated on the GPU with torch (same three classes
+    and proportions as precision_mix, a different random stream): a
+    (points // n, n) complex64 tensor."""
+    import math
+
+    import torch
+    g = torch.Generator(device=device).manual_seed(seed)
+    batch = points // n
+    out = torch.empty((batch, n), dtype=torch.complex64, device=device)
+    third = batch // 3
+    half = third + (batch - third) // 2
+    u = torch.rand((third, n, 2), generator=g, device=device) * 2 - 1
+    out[:third] = torch.view_as_complex(u.contiguous())
+    del u
+    mag = 10.0 ** (torch.rand((half - third, n), generator=g, device=device,
+                              dtype=torch.float64) * 6 - 3)
+    ph = torch.rand((half - third, n), generator=g, device=device,
+                    dtype=torch.float64) * (2 * math.pi)
+    out[third:half] = torch.polar(mag, ph).to(torch.complex64)
+    del mag, ph
+    bins = torch.randint(0, n, (batch - half, 1), generator=g, device=device)
+    j = torch.arange(n, device=device).unsqueeze(0)
+    turns = ((bins * j) % n).to(torch.float64) / n   # exact reduction of bin * j / n
+    out[half:] = torch.polar(torch.ones_like(turns), turns * (2 * math.pi)).to(torch.complex64)
+    return out

@@ -237,12 +237,33 @@ def test_sweep_in_place_sampled(n):
     a reduced batch; three transforms per call are checked against the
     oracle."""
     for bits in (32, 64):
-        if bits == 64 and n > (1 << 22):
-            continue
         batch = max(1, min(64, (1 << 22) // n))
         for direction in (-1, 1):
             _sweep_case(n, bits, batch, direction, inplace=True)
     _sweep_case(n, 32, max(1, min(8, (1 << 20) // n)), -1, inplace=False)
+
+
+def test_bench_config_rows_across_the_batch():
+    """The default benchmark workload itself: n = 4096, batch 16384 (2^26
+    points), in place, PRETUNED, device buffers, both directions.  Rows spread
+    over the whole batch, and every row of the last 32 (the last CTAs of the
+    launch), are checked against the long-double oracle."""
+    import torch
+    n, batch = 4096, 16384
+    x = oracle.uniform(n * batch, seed=n, dtype=np.complex64).reshape(batch, n)
+    rows = sorted(set(np.linspace(0, batch - 1, 64).astype(int).tolist()) |
+                  set(range(batch - 32, batch)))
+    d = torch.from_numpy(x).cuda()
+    for direction in (m.FORWARD, m.BACKWARD):
+        y = d.clone()
+        with m.Plan.create(n, direction, m.IN_PLACE, bits=32, batch=batch) as plan:
+            plan.execute(y, y)
+        torch.cuda.synchronize()
+        got = y[rows].cpu().numpy()
+        ref = oracle.fft_ld(x[rows].astype(np.complex128), direction)
+        assert rel_l2(got, ref) <= fp32_tol(n), direction
+        per = np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)
+        assert per.max() <= fp32_tol(n), (direction, int(np.argmax(per)))
 
 
 def test_every_specialised_kernel():

@@ -50,9 +50,12 @@ def test_mix_matches_oracle_host_and_device():
         st, lat = srv.wait(t)
         assert st == 0 and lat > 0
         torch.cuda.synchronize()
-        got = y.cpu().numpy()[:1]
-        ref = oracle.fft_ld(x.cpu().numpy()[:1].astype(np.complex128), d)
-        assert rel_l2(got, ref) <= (fp32_tol(n) if bits == 32 else fp64_tol(n)), (n, bits, d)
+        got = y.cpu().numpy()
+        ref = oracle.fft_ld(x.cpu().numpy().astype(np.complex128), d)
+        tol = fp32_tol(n) if bits == 32 else fp64_tol(n)
+        assert rel_l2(got, ref) <= tol, (n, bits, d)
+        for b in range(got.shape[0]):   # every transform of the request
+            assert rel_l2(got[b], ref[b]) <= tol, (n, bits, d, b)
     stats = srv.stats()
     assert stats["completed"] == 48 and stats["failed"] == 0
     srv.destroy()
@@ -83,6 +86,65 @@ def test_alone_equals_mix_and_coalesces(n):
     assert torch.equal(alone_out, mix_out)
     stats = srv.stats()
     assert stats["launches"] < len(tickets)       # requests were coalesced
+    srv.destroy()
+
+
+def test_alone_equals_mix_mixed_lengths_and_precisions():
+    """Each request of a stream that mixes lengths (one-pass and two-pass),
+    precisions, directions and host / device buffers gives bit-identical
+    results alone (the only request on the server) and in the mix, where
+    same-shape requests are coalesced into pointer-table launches and groups
+    of different shapes overlap on several streams."""
+    import torch
+    shapes = [(256, 32, -1), (1024, 64, 1), (4096, 32, -1), (65536, 32, -1),
+              (1 << 20, 32, 1), (512, 64, -1), (16384, 64, 1), (3 * 1024, 32, 1)]
+    probes = []
+    for k, (n, bits, d) in enumerate(shapes):
+        batch = 1 + k % 3
+        probes.append((n, bits, d, batch, _tensor(batch, n, bits, 500 + k), k % 4 == 3))
+
+    def submit(srv, n, bits, d, batch, x, host, keep):
+        if host:
+            hx = x.cpu().pin_memory()
+            hy = torch.empty_like(hx).pin_memory()
+            keep.append(hx)
+            return srv.submit(n, batch, d, bits, hx.data_ptr(), hy.data_ptr()), hy
+        y = torch.empty_like(x)
+        return srv.submit(n, batch, d, bits, x.data_ptr(), y.data_ptr()), y
+
+    alone = []
+    srv = m.Server(streams=2)
+    keep = []
+    for n, bits, d, batch, x, host in probes:
+        t, y = submit(srv, n, bits, d, batch, x, host, keep)
+        assert srv.wait(t)[0] == 0
+        torch.cuda.synchronize()
+        alone.append(y.cpu().clone())
+    srv.destroy()
+
+    srv = m.Server(streams=4)
+    tickets, mixed = [], {}
+    fillers = []
+    for rep in range(3):
+        for k, (n, bits, d, batch, x, host) in enumerate(probes):
+            if rep == 1:
+                mixed[k] = submit(srv, n, bits, d, batch, x, host, keep)
+                tickets.append(mixed[k][0])
+            fb = 1 + (rep + k) % 4
+            fx = _tensor(fb, n, bits, 900 + 10 * rep + k)
+            t, fy = submit(srv, n, bits, d, fb, fx, False, keep)
+            fillers.append((fx, fy))
+            tickets.append(t)
+    for t in tickets:
+        assert srv.wait(t)[0] == 0
+    torch.cuda.synchronize()
+    for k, (n, bits, d, batch, x, host) in enumerate(probes):
+        got = mixed[k][1].cpu()
+        assert torch.equal(got, alone[k]), (n, bits, d, host)
+        ref = oracle.fft_ld(x.cpu().numpy().astype(np.complex128), d)
+        tol = fp32_tol(n) if bits == 32 else fp64_tol(n)
+        assert rel_l2(got.numpy(), ref) <= tol, (n, bits, d)
+    assert srv.stats()["launches"] < len(tickets)
     srv.destroy()
 
 
