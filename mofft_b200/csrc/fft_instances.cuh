@@ -14,6 +14,10 @@ struct Entry {
   mofft_kernel_desc desc;
   launch_fn launch;
   func_fn func;
+  // kernels with a constant table of their own (e.g. DFT-matrix operands):
+  // its size and its host-side construction; 0 / null for the others
+  size_t aux_bytes;
+  int (*fill_aux)(void *dst);
 };
 
 template <typename T>
@@ -278,5 +282,6 @@ const Entry *entries_cols_f64(int *count);
 const Entry *entries_rows_mixed(int *count);
 const Entry *entries_cols_mixed(int *count);
 const Entry *entries_tensor(int *count);
+const Entry *entries_tensor64(int *count);
 
 }  // namespace mofft

@@ -16,7 +16,8 @@ const std::vector<Entry> &registry() {
     const Entry *(*lists[])(int *) = {entries_generic, entries_rows_f32,
                                       entries_rows_f64, entries_cols_f32,
                                       entries_cols_f64, entries_rows_mixed,
-                                      entries_cols_mixed, entries_tensor};
+                                      entries_cols_mixed, entries_tensor64,
+                                      entries_tensor};
     for (auto list : lists) {
       int n = 0;
       const Entry *e = list(&n);
@@ -52,6 +53,19 @@ extern "C" int mofft_cuda_prepare_device(void) {
     if (err != cudaSuccess) return (int)err;
   }
   return 0;
+}
+
+extern "C" size_t mofft_cuda_kernel_aux_bytes(int kernel) {
+  const auto &r = registry();
+  if (kernel < 0 || kernel >= (int)r.size()) return 0;
+  return r[kernel].fill_aux ? r[kernel].aux_bytes : 0;
+}
+
+extern "C" int mofft_cuda_kernel_fill_aux(int kernel, void *dst) {
+  const auto &r = registry();
+  if (kernel < 0 || kernel >= (int)r.size() || !r[kernel].fill_aux || !dst)
+    return (int)cudaErrorInvalidValue;
+  return r[kernel].fill_aux(dst);
 }
 
 extern "C" int mofft_cuda_launch_pass(int kernel, const mofft_pass_args *args,

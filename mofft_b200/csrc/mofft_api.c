@@ -638,7 +638,10 @@ static mofft_status materialise_schedule(mofft_core *c) {
     ps->aux_offset = ps->status_offset = 0;
     if (is_tensor_kind(ps->kind)) {
       ps->aux_offset = bytes;
-      bytes = align256(bytes + mofft_cuda_tensor_aux_bytes(mofft_cuda_kernel_get(ps->kernel)->form));
+      const size_t own = mofft_cuda_kernel_aux_bytes(ps->kernel);
+      bytes = align256(bytes + (own ? own
+                                    : mofft_cuda_tensor_aux_bytes(
+                                          mofft_cuda_kernel_get(ps->kernel)->form)));
     }
     if (pass_has_status(ps)) {
       ps->status_offset = bytes;
@@ -659,7 +662,12 @@ static mofft_status materialise_schedule(mofft_core *c) {
       mofft_write_twiddles(host + ps->tw_hi_offset, c->precision_bits, m, 0, lo_n, hi_n);
       mofft_write_twiddles(host + ps->tw_lo_offset, c->precision_bits, m, 0, 1, lo_n);
     }
-    if (is_tensor_kind(ps->kind)) {
+    if (is_tensor_kind(ps->kind) && mofft_cuda_kernel_aux_bytes(ps->kernel)) {
+      if (mofft_cuda_kernel_fill_aux(ps->kernel, host + ps->aux_offset) != 0) {
+        free(host);
+        return MOFFT_INTERNAL_ERROR;
+      }
+    } else if (is_tensor_kind(ps->kind)) {
       double fr[256], fi[256];
       for (int k = 0; k < 16; ++k)
         for (int r = 0; r < 16; ++r) {

@@ -89,6 +89,11 @@ int mofft_cuda_prepare_device(void);
 size_t mofft_cuda_tensor_aux_bytes(int form);
 int mofft_cuda_tensor_fill_aux(int form, void *dst, const double *fr,
                                const double *fi);
+/* Kernels that carry a constant table of their own (the radix-64 tensor-core
+ * kernel: DFT-matrix operand tiles and twiddles): its size in bytes (0 for
+ * every other kernel) and its host-side construction into dst. */
+size_t mofft_cuda_kernel_aux_bytes(int kernel);
+int mofft_cuda_kernel_fill_aux(int kernel, void *dst);
 /* Launch one pass on `stream` (a cudaStream_t).  Returns a cudaError_t. */
 int mofft_cuda_launch_pass(int kernel, const mofft_pass_args *args,
                            void *stream);

@@ -107,13 +107,14 @@ def test_schedule_switch_and_unsupported_length():
     kernels = {k["index"]: k for k in m.kernels()}
     tensor = [k for k in kernels.values() if k["kind"] == m.KERNEL_TENSOR]
     assert sorted(k["name"] for k in tensor) == ["tensor_float_4096_bf16x3_r16x3",
+                                                "tensor_float_4096_bf16x3_r64x2",
                                                 "tensor_float_4096_tf32x3_r16x3"]
     with m.Plan.create(N, m.FORWARD, m.OUT_OF_PLACE, bits=32, batch=4) as plan:
         base = plan.schedule()
         plan.set_precision_form(m.FORM_BF16X3)
         s = plan.schedule()
         assert s["pass_count"] == 1
-        assert kernels[s["kernels"][0]]["name"] == "tensor_float_4096_bf16x3_r16x3"
+        assert kernels[s["kernels"][0]]["name"] == "tensor_float_4096_bf16x3_r64x2"
         plan.set_precision_form(m.FORM_FP32)
         assert plan.schedule()["kernels"] == base["kernels"]
     with m.Plan.create(2048, m.FORWARD, m.OUT_OF_PLACE, bits=32, batch=4) as plan:
@@ -247,11 +248,13 @@ def test_precision_config_full_size_sampled(n):
                                            for f, e in errs.items()})
 
 
-def test_lost_copy_times_out_and_plan_stays_usable():
-    """The tensor-core kernel bounds every wait: a launch whose input copies
-    are never issued ends in MOFFT_INTERNAL_ERROR after about a second per
-    CTA (no GPU fault, TMEM released), and the same plan then executes
-    correctly on the same context."""
+@pytest.mark.parametrize("form", [m.FORM_TF32X3, m.FORM_BF16X3])
+def test_lost_copy_times_out_and_plan_stays_usable(form):
+    """The tensor-core kernels bound every wait: a launch whose first wait
+    can never be satisfied (radix-16 kernel: the input copies are never
+    issued; radix-64 kernel: the first GEMM is never issued) ends in
+    MOFFT_INTERNAL_ERROR after about a second (no GPU fault, TMEM released),
+    and the same plan then executes correctly on the same context."""
     import ctypes
     import time
     import torch
@@ -263,7 +266,7 @@ def test_lost_copy_times_out_and_plan_stays_usable():
     with m.Plan.create(N, m.FORWARD, m.OUT_OF_PLACE, bits=32, batch=8) as plan:
         assert lib.mofft_plan_check_lost_copy_f32(plan.handle, d.data_ptr(), out.data_ptr()) \
             == m.Status.INVALID_ARGUMENT          # CUDA-core schedule: nothing to check
-        plan.set_precision_form(m.FORM_TF32X3)
+        plan.set_precision_form(form)
         t0 = time.perf_counter()
         st = lib.mofft_plan_check_lost_copy_f32(plan.handle, d.data_ptr(), out.data_ptr())
         waited = time.perf_counter() - t0
@@ -271,4 +274,4 @@ def test_lost_copy_times_out_and_plan_stays_usable():
         assert waited < 30.0, waited
         plan.check_status()                       # the error word was cleared
         plan.execute(d, out)
-    assert rel_l2(out.cpu().numpy(), want) <= TOL[m.FORM_TF32X3]
+    assert rel_l2(out.cpu().numpy(), want) <= TOL[form]

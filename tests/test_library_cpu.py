@@ -272,6 +272,7 @@ def test_tensor_forms_registered_and_never_planned():
     tensor = sorted((k["name"], k["length"], k["radices"], k["precision_bits"])
                     for k in ks if k["kind"] == m.KERNEL_TENSOR)
     assert tensor == [("tensor_float_4096_bf16x3_r16x3", 4096, [16, 16, 16], 32),
+                      ("tensor_float_4096_bf16x3_r64x2", 4096, [64, 64], 32),
                       ("tensor_float_4096_tf32x3_r16x3", 4096, [16, 16, 16], 32)]
     cols = sorted((k["name"], k["length"], k["lines"], k["radices"])
                   for k in ks if k["kind"] == m.KERNEL_TENSOR_COLS)
