@@ -13,6 +13,9 @@ const Entry *entries_cols_f32(int *count) {
       COLS(float, 1024, 64, 8, 16, 16, 4),
       COLS(float, 2048, 64, 8, 16, 16, 8),
       COLS(float, 4096, 128, 4, 16, 16, 16),
+      COLS(float, 1024, 32, 16, 16, 16, 4),
+      COLS(float, 2048, 128, 8, 16, 16, 8),
+      COLS(float, 4096, 256, 4, 16, 16, 16),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;
