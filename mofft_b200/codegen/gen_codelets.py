@@ -21,6 +21,31 @@ Algebra used (restated from the published methods, not from any library):
     compile-time twiddles; multiplications by 1, -1, +-i are folded and
     multiplications by (+-1 +- i)/sqrt(2) use two real multiplies.
 
+Rewrite families.  Besides the default codelet above, every radix gets one
+codelet per algebraic rewrite the reference's compiler defines for it
+(``rewrites.py:15-41``: DIRECT and LIKE_TERMS for every radix, EVEN_ODD and
+LIKE_TERMS_EVEN_ODD for even radices, VECTOR_REUSE and
+LIKE_TERMS_VECTOR_REUSE for radices divisible by four), each a different
+straight-line evaluation order of the same DFT:
+  * direct:       y_k = sum_j x_j W^jk, one complex linear form per output;
+  * like_terms:   conjugate pairs a_j = x_j + x_{R-j}, b_j = x_j - x_{R-j}
+                  (and the middle element of an even radix), outputs k and
+                  R - k from the same two partial sums;
+  * even_odd:     E_k (even j) and O_k (odd j) for k < R/2, then
+                  y_k = E_k + O_k and y_{k+R/2} = E_k - O_k;
+  * like_terms_even_odd: E_k and O_k each from conjugate pairs of one parity;
+  * vector_reuse: for s < R/4, the sums S_r of x_j W^js over j = r mod 4 and
+                  the four outputs y_{s + qR/4} = sum_r S_r (-i)^(rq), so the
+                  coefficients of the first quarter are reused (a radix-4
+                  butterfly on the partial sums);
+  * like_terms_vector_reuse: the same with conjugate pairs in the residue
+                  classes 0 and 2 (j and R - j fall in the same class there).
+``DftFamily<R, F>`` selects one; ``BankDft<R, BANK>`` is the codelet kernel
+bank BANK runs (0 default, 1 like_terms, 2 like_terms_even_odd where the
+radix is even, 3 like_terms_vector_reuse where it is divisible by four; the
+default codelet where the bank's family is not defined, and for radix 32 and
+64 stages, whose matrix forms would not fit a thread's registers).
+
 Run:  python -m mofft_b200.codegen.gen_codelets <out_dir>
 It writes ``codelets.cuh`` (device code) and ``codelet_costs.h`` (real add /
 multiply counts per radix, used by the host cost model).
@@ -231,6 +256,196 @@ class Emitter:
         return ys
 
 
+    # ---------------------------------------------------------- families
+    def linear(self, xs, coeffs):
+        """sum_j coeffs[j] * xs[j] for compile-time complex coefficients
+        (real, imaginary) pairs; zero and unit parts fold away."""
+        eps = 1e-14
+        re_terms, im_terms = [], []
+        muls = 0
+        for x, (c, s) in zip(xs, coeffs):
+            # c * (xr + i xi) contributes (c xr, c xi); i s * x gives (-s xi, s xr)
+            for coef, part_re, part_im in ((c, x[0], x[1]), (s, f"-{x[1]}", x[0])):
+                if abs(coef) < eps:
+                    continue
+                if abs(coef - 1) < eps:
+                    re_terms.append(part_re)
+                    im_terms.append(part_im)
+                elif abs(coef + 1) < eps:
+                    re_terms.append(f"-({part_re})")
+                    im_terms.append(f"-({part_im})")
+                else:
+                    lit = _lit(coef)
+                    re_terms.append(f"({part_re}) * {lit}")
+                    im_terms.append(f"({part_im}) * {lit}")
+                    muls += 2
+        if not re_terms:
+            return (self.tmp("T(0)"), self.tmp("T(0)"))
+        adds = len(re_terms) - 1
+        return (self.tmp(" + ".join(re_terms), adds, muls // 2),
+                self.tmp(" + ".join(im_terms), adds, muls - muls // 2))
+
+    def _w(self, j: int, k: int, radix: int):
+        """Forward coefficient W^jk = cos - i sin of 2 pi jk / R."""
+        c, s = cis_turns(j * k, radix)
+        return (c, -s)
+
+    def family(self, xs, fam: str):
+        radix = len(xs)
+        if fam == "direct":
+            return [self.linear(xs, [self._w(j, k, radix) for j in range(radix)])
+                    for k in range(radix)]
+        if fam == "like_terms":
+            return self._like_terms(xs)
+        if fam in ("even_odd", "like_terms_even_odd"):
+            half = radix // 2
+            ys = [None] * radix
+            if fam == "even_odd":
+                evens = list(range(0, radix, 2))
+                odds = list(range(1, radix, 2))
+                for k in range(half):
+                    e = self.linear([xs[j] for j in evens], [self._w(j, k, radix) for j in evens])
+                    o = self.linear([xs[j] for j in odds], [self._w(j, k, radix) for j in odds])
+                    ys[k] = self.add(e, o)
+                    ys[k + half] = self.sub(e, o)
+                return ys
+            pairs = self._pairs(xs)
+            for k in range(half):
+                e = self._paired_sum(xs, pairs, k, parity=0)
+                o = self._paired_sum(xs, pairs, k, parity=1)
+                ys[k] = self.add(e, o)
+                ys[k + half] = self.sub(e, o)
+            return ys
+        if fam in ("vector_reuse", "like_terms_vector_reuse"):
+            q = radix // 4
+            pairs = self._pairs(xs) if fam == "like_terms_vector_reuse" else None
+            ys = [None] * radix
+            for s_ in range(q):
+                sums = []
+                for r in range(4):
+                    if pairs is not None and r in (0, 2):
+                        sums.append(self._paired_sum(xs, pairs, s_, residue=r))
+                    else:
+                        js = [j for j in range(radix) if j % 4 == r]
+                        sums.append(self.linear([xs[j] for j in js],
+                                                [self._w(j, s_, radix) for j in js]))
+                s0, s1, s2, s3 = sums
+                a02, d02 = self.add(s0, s2), self.sub(s0, s2)
+                a13, d13 = self.add(s1, s3), self.sub(s1, s3)
+                mi = (self.tmp(f"{d13[1]}"), self.tmp(f"-{d13[0]}"))   # -i (s1 - s3)
+                ys[s_] = self.add(a02, a13)
+                ys[s_ + q] = self.add(d02, mi)
+                ys[s_ + 2 * q] = self.sub(a02, a13)
+                ys[s_ + 3 * q] = self.sub(d02, mi)
+            return ys
+        raise ValueError(fam)
+
+    def _pairs(self, xs):
+        """a_j = x_j + x_{R-j}, b_j = x_j - x_{R-j} for 1 <= j < R/2."""
+        radix = len(xs)
+        out = {}
+        for j in range(1, (radix + 1) // 2):
+            out[j] = (self.add(xs[j], xs[radix - j]), self.sub(xs[j], xs[radix - j]))
+        return out
+
+    def _paired_sum(self, xs, pairs, k, parity=None, residue=None):
+        """sum over j of x_j W^jk (the pairs j, R-j together) restricted to
+        j of one parity or one residue mod 4: x_j W^jk + x_{R-j} W^-jk =
+        a_j cos - i b_j sin."""
+        radix = len(xs)
+
+        def keep(j):
+            if parity is not None:
+                return j % 2 == parity
+            if residue is not None:
+                return j % 4 == residue
+            return True
+        terms, coeffs = [], []
+        if keep(0):
+            terms.append(xs[0])
+            coeffs.append((1.0, 0.0))
+        if radix % 2 == 0 and keep(radix // 2):
+            terms.append(xs[radix // 2])
+            coeffs.append(self._w(radix // 2, k, radix))
+        for j, (a, b) in pairs.items():
+            if not keep(j):
+                continue
+            c, s = cis_turns(j * k, radix)
+            terms.append(a)
+            coeffs.append((c, 0.0))
+            terms.append(b)
+            coeffs.append((0.0, -s))
+        return self.linear(terms, coeffs)
+
+    def _like_terms(self, xs):
+        radix = len(xs)
+        pairs = self._pairs(xs)
+        ys = [None] * radix
+        ys[0] = self._paired_sum(xs, pairs, 0)
+        for k in range(1, radix // 2 + 1):
+            # C_k: x_0, middle and a_j cos; S_k: b_j sin.  y_k = C - i S,
+            # y_{R-k} = C + i S
+            cterms, ccoef = [xs[0]], [(1.0, 0.0)]
+            if radix % 2 == 0:
+                cterms.append(xs[radix // 2])
+                ccoef.append(self._w(radix // 2, k, radix))
+            sterms, scoef = [], []
+            for j, (a, b) in pairs.items():
+                c, s_ = cis_turns(j * k, radix)
+                cterms.append(a)
+                ccoef.append((c, 0.0))
+                sterms.append(b)
+                scoef.append((s_, 0.0))
+            cc = self.linear(cterms, ccoef)
+            ss = self.linear(sterms, scoef) if sterms else (self.tmp("T(0)"), self.tmp("T(0)"))
+            if 2 * k == radix:
+                ys[k] = cc
+            else:
+                ys[k] = (self.tmp(f"{cc[0]} + {ss[1]}", 1), self.tmp(f"{cc[1]} - {ss[0]}", 1))
+                ys[radix - k] = (self.tmp(f"{cc[0]} - {ss[1]}", 1),
+                                 self.tmp(f"{cc[1]} + {ss[0]}", 1))
+        return ys
+
+
+FAMILIES = ("direct", "like_terms", "even_odd", "like_terms_even_odd", "vector_reuse",
+            "like_terms_vector_reuse")
+FAMILY_ID = {name: i + 1 for i, name in enumerate(FAMILIES)}   # 0 = default codelet
+# codelet family per kernel bank (the default codelet where it is not defined)
+BANK_FAMILIES = {1: ("like_terms",), 2: ("like_terms_even_odd",),
+                 3: ("like_terms_vector_reuse",)}
+BANK_COUNT = 4
+
+
+def family_defined(radix: int, fam: str) -> bool:
+    """rewrites.py:24-41: which rewrites are defined for a radix."""
+    if fam in ("direct", "like_terms"):
+        return True
+    if fam in ("even_odd", "like_terms_even_odd"):
+        return radix % 2 == 0
+    return radix % 4 == 0
+
+
+def bank_family(radix: int, bank: int) -> str | None:
+    for fam in BANK_FAMILIES.get(bank, ()):
+        if family_defined(radix, fam):
+            return fam
+    return None
+
+
+def emit_family(radix: int, fam: str) -> str:
+    em = Emitter()
+    xs = [(f"re[{j}]", f"im[{j}]") for j in range(radix)]
+    loaded = [(em.tmp(x[0]), em.tmp(x[1])) for x in xs]
+    ys = em.family(loaded, fam)
+    body = list(em.lines)
+    for k, (yr, yi) in enumerate(ys):
+        body.append(f"  re[{k}] = {yr};")
+        body.append(f"  im[{k}] = {yi};")
+    return (f"template <typename T>\n"
+            f"__device__ __forceinline__ void dft_fwd_{radix}_{fam}(T (&re)[{radix}], "
+            f"T (&im)[{radix}]) {{\n" + "\n".join(body) + "\n}\n")
+
+
 def emit_radix(radix: int) -> tuple[str, int, int]:
     em = Emitter()
     xs = []
@@ -269,6 +484,33 @@ def generate() -> tuple[str, str]:
             f"__device__ __forceinline__ static void fwd(T (&re)[{radix}], "
             f"T (&im)[{radix}]) {{ dft_fwd_{radix}(re, im); }} }};")
     parts.append("\n".join(dispatch) + "\n")
+    # rewrite families
+    for radix in RADICES:
+        for fam in FAMILIES:
+            if family_defined(radix, fam):
+                parts.append(emit_family(radix, fam))
+    fam_lines = ["// Codelet of rewrite family F (1-based index into " +
+                 ", ".join(FAMILIES) + ").",
+                 "template <int R, int F> struct DftFamily;"]
+    for radix in RADICES:
+        for fam in FAMILIES:
+            if family_defined(radix, fam):
+                fam_lines.append(
+                    f"template <> struct DftFamily<{radix}, {FAMILY_ID[fam]}> {{ "
+                    f"template <typename T> __device__ __forceinline__ static void "
+                    f"fwd(T (&re)[{radix}], T (&im)[{radix}]) {{ "
+                    f"dft_fwd_{radix}_{fam}(re, im); }} }};")
+    fam_lines.append("// Codelet kernel bank B runs for radix R (families for radices up to 16;")
+    fam_lines.append("// radix-32 and -64 stages keep the split codelet in every bank).")
+    fam_lines.append("template <int R, int B> struct BankDft : Dft<R> {};")
+    for radix in (r for r in RADICES if r <= 16):
+        for bank in range(1, BANK_COUNT):
+            fam = bank_family(radix, bank)
+            if fam is not None:
+                fam_lines.append(
+                    f"template <> struct BankDft<{radix}, {bank}> : "
+                    f"DftFamily<{radix}, {FAMILY_ID[fam]}> {{}};")
+    parts.append("\n".join(fam_lines) + "\n")
     cost_lines = [
         "// Generated by mofft_b200/codegen/gen_codelets.py -- do not edit.",
         "// Real additions / multiplications of one forward radix-R codelet.",

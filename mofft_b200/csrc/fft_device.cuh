@@ -1002,7 +1002,7 @@ struct GenericArgs {
   T sign_out;
 };
 
-template <typename T, int R>
+template <typename T, int R, int BANK>
 __device__ __forceinline__ void generic_butterfly(
     const GenericArgs<T>& a, const T* __restrict__ sre_src,
     const T* __restrict__ sim_src, T* __restrict__ sre_dst,
@@ -1052,7 +1052,7 @@ __device__ __forceinline__ void generic_butterfly(
       cmul<T>(vr[r], vi[r], w.x, w.y);
     }
   }
-  Dft<R>::fwd(vr, vi);
+  BankDft<R, BANK>::fwd(vr, vi);
   const int base = (j / NS) * NS * R + (j % NS);
 #pragma unroll
   for (int k = 0; k < R; ++k) {
@@ -1077,14 +1077,14 @@ __device__ __forceinline__ void generic_butterfly(
 // WIDE selects the variant that also handles radix 32 and 64; chains without
 // them use the narrow variant, whose register footprint allows several CTAs
 // per SM.
-template <typename T, bool WIDE>
+template <typename T, bool WIDE, int BANK>
 __device__ __forceinline__ void generic_dispatch(
     int R, const GenericArgs<T>& a, const T* sre_src, const T* sim_src,
     T* sre_dst, T* sim_dst, int line, int j, int L, int NS, int twoff,
     bool first, bool last, int line_words, long long b, long long jline) {
 #define MOFFT_GENERIC_CASE(RR)                                                  \
   case RR:                                                                      \
-    generic_butterfly<T, RR>(a, sre_src, sim_src, sre_dst, sim_dst, line, j, L, \
+    generic_butterfly<T, RR, BANK>(a, sre_src, sim_src, sre_dst, sim_dst, line, j, L, \
                              NS, twoff, first, last, line_words, b, jline);     \
     break;
   switch (R) {
@@ -1096,10 +1096,10 @@ __device__ __forceinline__ void generic_dispatch(
     default:
       if (WIDE) {
         if (R == 32)
-          generic_butterfly<T, 32>(a, sre_src, sim_src, sre_dst, sim_dst, line, j, L,
+          generic_butterfly<T, 32, BANK>(a, sre_src, sim_src, sre_dst, sim_dst, line, j, L,
                                    NS, twoff, first, last, line_words, b, jline);
         else if (R == 64)
-          generic_butterfly<T, 64>(a, sre_src, sim_src, sre_dst, sim_dst, line, j, L,
+          generic_butterfly<T, 64, BANK>(a, sre_src, sim_src, sre_dst, sim_dst, line, j, L,
                                    NS, twoff, first, last, line_words, b, jline);
       }
       break;
@@ -1107,7 +1107,9 @@ __device__ __forceinline__ void generic_dispatch(
 #undef MOFFT_GENERIC_CASE
 }
 
-template <typename T, bool WIDE>
+// BANK: the kernel bank whose codelets the stages run (0 default, 1-3 the
+// rewrite families of BankDft).
+template <typename T, bool WIDE, int BANK>
 __global__ void __launch_bounds__(256, WIDE ? 1 : 2) generic_kernel(const GenericArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int L = a.length;
@@ -1150,7 +1152,7 @@ __global__ void __launch_bounds__(256, WIDE ? 1 : 2) generic_kernel(const Generi
       const long long bb = cols ? b : b + line;
       if (bb >= a.batch) continue;
       const long long jline = cols ? jfirst + line : 0;
-      generic_dispatch<T, WIDE>(R, a, bufs[cur][0], bufs[cur][1], bufs[cur ^ 1][0],
+      generic_dispatch<T, WIDE, BANK>(R, a, bufs[cur][0], bufs[cur][1], bufs[cur ^ 1][0],
                           bufs[cur ^ 1][1], line, j, L, NS, twoff, first, last,
                           line_words, cols ? b : bb, jline);
     }

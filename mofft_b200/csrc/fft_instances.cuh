@@ -176,10 +176,10 @@ size_t generic_smem(int L, int lines, int cols) {
   return 4 * words * sizeof(T);
 }
 
-template <typename T, bool WIDE>
+template <typename T, bool WIDE, int BANK = 0>
 struct GenericInst {
   static const void *func() {
-    return reinterpret_cast<const void *>(&generic_kernel<T, WIDE>);
+    return reinterpret_cast<const void *>(&generic_kernel<T, WIDE, BANK>);
   }
   static cudaError_t launch(const mofft_pass_args *p, cudaStream_t s) {
     GenericArgs<T> a;
@@ -223,12 +223,13 @@ struct GenericInst {
     if (grid <= 0) return cudaSuccess;
     if (grid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     const size_t smem = generic_smem<T>(p->length, p->lines, p->generic_cols);
-    generic_kernel<T, WIDE><<<(unsigned)grid, 256, smem, s>>>(a);
+    generic_kernel<T, WIDE, BANK><<<(unsigned)grid, 256, smem, s>>>(a);
     return cudaGetLastError();
   }
   static Entry entry(const char *name) {
     Entry e{};
     e.desc.name = name;
+    e.desc.bank = BANK;
     e.desc.precision_bits = sizeof(T) == 4 ? 32 : 64;
     e.desc.kind = MOFFT_KERNEL_GENERIC;
     e.desc.length = 0;

@@ -208,7 +208,10 @@ int mofft_ceil_log2_u64(uint64_t x) {
 
 /* Generic (runtime stage list) kernel that can run every radix of `chain`:
  * the narrow variant (radix <= 16) when possible, else the wide one. */
-static int generic_kernel_index(int precision_bits, const int *chain, int count) {
+/* Runtime-stage kernel of kernel bank `bank` (its codelet family) whose
+ * largest radix covers the chain: the narrow variant when it suffices. */
+static int generic_kernel_index(int precision_bits, unsigned bank, const int *chain,
+                                int count) {
   int max_radix = 0;
   for (int i = 0; i < count; ++i)
     if (chain[i] > max_radix) max_radix = chain[i];
@@ -216,7 +219,9 @@ static int generic_kernel_index(int precision_bits, const int *chain, int count)
   const int n = mofft_cuda_kernel_count();
   for (int i = 0; i < n; ++i) {
     const mofft_kernel_desc *d = mofft_cuda_kernel_get(i);
-    if (d->kind != MOFFT_KERNEL_GENERIC || d->precision_bits != precision_bits) continue;
+    if (d->kind != MOFFT_KERNEL_GENERIC || d->precision_bits != precision_bits ||
+        d->bank != (int)bank)
+      continue;
     const int cap = d->radices[0];
     if (cap >= max_radix && cap < best_cap) {
       best = i;
@@ -344,7 +349,7 @@ static int make_pass(int precision_bits, unsigned bank, const int *chain,
       return 1;
     }
   }
-  const int g = generic_kernel_index(precision_bits, chain + begin, count);
+  const int g = generic_kernel_index(precision_bits, bank, chain + begin, count);
   if (g < 0) return 0;
   int lines = single ? generic_rows_lines(precision_bits, (int)length)
                      : generic_cols_lines(precision_bits, (int)length, total,

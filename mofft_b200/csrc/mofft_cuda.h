@@ -39,6 +39,9 @@ typedef struct {
   int form;             /* mofft_precision_form; 0 for the CUDA-core kernels */
   int prefetch;         /* ROWS: persistent CTAs that bulk-copy the next line
                            (the pass takes an error word, `status`) */
+  int bank;             /* kernel bank whose codelets it runs: 0 default,
+                           1 like-terms, 2 even-odd, 3 vector-reuse families
+                           (runtime-stage kernels) */
 } mofft_kernel_desc;
 
 typedef struct {

@@ -78,7 +78,11 @@ mofft_status mofft_search_best(mofft_core **out, int precision_bits,
 int mofft_wisdom_lookup(size_t length, int precision_bits, int *chain,
                         int capacity, int *preferred);
 
-#define MOFFT_KERNEL_BANK_COUNT 2u
+/* Kernel banks (the reference's compiled code families, portfolio.py:31-35):
+ * 0 the specialised kernels with the default codelets (runtime-stage kernels
+ * where none is specialised), 1-3 the runtime-stage kernels with the
+ * like-terms, even-odd and vector-reuse rewrite codelets. */
+#define MOFFT_KERNEL_BANK_COUNT 4u
 
 #ifdef __cplusplus
 }

@@ -27,18 +27,28 @@ template <typename T, int R> void run(const double* in, double* out) {
   Dft<R>::fwd(re, im);
   for (int i = 0; i < R; ++i) { out[2*i] = (double)re[i]; out[2*i+1] = (double)im[i]; }
 }
-template <typename T> void dispatch(int R, const double* in, double* out) {
-  switch (R) {
+template <typename T, int R, int F> void runf(const double* in, double* out) {
+  T re[R], im[R];
+  for (int i = 0; i < R; ++i) { re[i] = (T)in[2*i]; im[i] = (T)in[2*i+1]; }
+  DftFamily<R, F>::fwd(re, im);
+  for (int i = 0; i < R; ++i) { out[2*i] = (double)re[i]; out[2*i+1] = (double)im[i]; }
+}
+template <typename T> void dispatch(int R, int F, const double* in, double* out) {
+  if (F == 0) {
+    switch (R) {
 #define C(RR) case RR: run<T, RR>(in, out); break;
-    C(2) C(3) C(4) C(5) C(6) C(7) C(8) C(9) C(10) C(11) C(12) C(13) C(14) C(15) C(16) C(32) C(64)
+      C(2) C(3) C(4) C(5) C(6) C(7) C(8) C(9) C(10) C(11) C(12) C(13) C(14) C(15) C(16) C(32) C(64)
+    }
+    return;
   }
+FAMILY_DISPATCH
 }
 int main(int argc, char** argv) {
-  int bits, R;
+  int bits, R, F;
   double in[128], out[128];
-  while (scanf("%d %d", &bits, &R) == 2) {
+  while (scanf("%d %d %d", &bits, &R, &F) == 3) {
     for (int i = 0; i < 2 * R; ++i) if (scanf("%lf", &in[i]) != 1) return 1;
-    if (bits == 32) dispatch<float>(R, in, out); else dispatch<double>(R, in, out);
+    if (bits == 32) dispatch<float>(R, F, in, out); else dispatch<double>(R, F, in, out);
     for (int i = 0; i < 2 * R; ++i) printf("%.17g ", out[i]);
     printf("\n");
   }
@@ -52,7 +62,14 @@ def harness(tmp_path_factory):
     d = tmp_path_factory.mktemp("codelets")
     cuh, _ = gen_codelets.generate()
     (d / "codelets.cuh").write_text(cuh)
-    (d / "h.cpp").write_text(HARNESS)
+    fam = []
+    for radix in RADICES:
+        for name in gen_codelets.FAMILIES:
+            if gen_codelets.family_defined(radix, name):
+                f = gen_codelets.FAMILY_ID[name]
+                fam.append(f"  if (R == {radix} && F == {f}) {{ runf<T, {radix}, {f}>(in, out); "
+                           "return; }")
+    (d / "h.cpp").write_text(HARNESS.replace("FAMILY_DISPATCH", "\n".join(fam)))
     exe = d / "h"
     subprocess.run(["g++", "-O1", "-std=c++17", "-ffp-contract=off", "-o", str(exe),
                     str(d / "h.cpp")], check=True, cwd=d)
@@ -61,9 +78,11 @@ def harness(tmp_path_factory):
 
 def run_cases(exe: Path, cases):
     lines = []
-    for bits, x in cases:
+    for case in cases:
+        bits, x = case[0], case[1]
+        fam = case[2] if len(case) > 2 else 0
         vals = " ".join(f"{v:.17g}" for z in x for v in (z.real, z.imag))
-        lines.append(f"{bits} {len(x)} {vals}")
+        lines.append(f"{bits} {len(x)} {fam} {vals}")
     out = subprocess.run([str(exe)], input="\n".join(lines) + "\n", capture_output=True,
                          text=True, check=True).stdout.strip().splitlines()
     res = []
@@ -100,6 +119,53 @@ def test_codelets_match_reference_evaluator(harness, golden_codelets):
             y = np.conj(y)
         tol = 64 * FLT_EPS * radix if bits == 32 else 192 * DBL_EPS * radix
         assert np.max(np.abs(y - want)) <= tol, (stem, bits)
+
+
+def test_rewrite_family_codelets_match_reference_evaluator(harness, golden_codelets):
+    """Every (radix, rewrite family) codelet the generator emits, both
+    directions, FP32 and FP64, against the reference's evaluate_pattern
+    output for that radix and pattern (rewrites.py:43-95)."""
+    cases, wants, meta = [], [], []
+    seen = set()
+    for radix in RADICES:
+        for name in gen_codelets.FAMILIES:
+            if not gen_codelets.family_defined(radix, name):
+                continue
+            for direction in ("forward", "backward"):
+                stem = f"r{radix}_{direction}_{name}"
+                assert stem + "_in" in golden_codelets.files, stem
+                x = golden_codelets[stem + "_in"]
+                want = golden_codelets[stem + "_out"]
+                backward = direction == "backward"
+                for bits in (32, 64):
+                    cases.append((bits, np.conj(x) if backward else x,
+                                  gen_codelets.FAMILY_ID[name]))
+                    wants.append(want)
+                    meta.append((stem, bits, radix, backward))
+                seen.add((radix, name))
+    outs = run_cases(harness, cases)
+    assert len(outs) == len(cases)
+    for y, want, (stem, bits, radix, backward) in zip(outs, wants, meta):
+        if backward:
+            y = np.conj(y)
+        tol = 64 * FLT_EPS * radix if bits == 32 else 192 * DBL_EPS * radix
+        assert np.max(np.abs(y - want)) <= tol, (stem, bits)
+    # every pattern the reference defines for each radix is covered
+    assert len(seen) == sum(1 for r in RADICES for n in gen_codelets.FAMILIES
+                            if gen_codelets.family_defined(r, n))
+    assert (64, "like_terms_vector_reuse") in seen and (3, "like_terms") in seen
+
+
+def test_bank_codelet_choice():
+    """Kernel banks follow the reference's portfolio families
+    (portfolio.py:31-35): 1 like-terms, 2 even-odd, 3 vector-reuse, the
+    default codelet where a bank's family is not defined for the radix."""
+    assert gen_codelets.BANK_COUNT == 4
+    assert gen_codelets.bank_family(5, 1) == "like_terms"
+    assert gen_codelets.bank_family(6, 2) == "like_terms_even_odd"
+    assert gen_codelets.bank_family(5, 2) is None
+    assert gen_codelets.bank_family(8, 3) == "like_terms_vector_reuse"
+    assert gen_codelets.bank_family(6, 3) is None
 
 
 def test_constants_correctly_rounded():

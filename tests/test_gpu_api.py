@@ -59,7 +59,7 @@ def test_measured_planner():
                                                           ctypes.byref(d))
                 assert st == 0
                 assert d.measured == 1 and 1 <= d.candidates_measured <= 4
-                assert d.kernel_bank < d.kernel_bank_count == 2
+                assert d.kernel_bank < d.kernel_bank_count == 4
                 assert d.selected_median_seconds > 0 and d.planning_seconds > 0
                 assert d.length == TEST_N and d.precision_bits == bits
                 assert int(np.prod(d.radix_list())) == TEST_N
@@ -132,7 +132,7 @@ def test_pretuned_strict_and_bound_api():
 def test_each_kernel_bank():
     """test_each_compiled_bank (tests/test_planning.c:254-302): chain {3, 10}."""
     radices = (ctypes.c_int * 2)(3, 10)
-    for bank in (0, 1):
+    for bank in (0, 1, 2, 3):   # default codelets, like-terms, even-odd, vector-reuse
         for direction in (m.FORWARD, m.BACKWARD):
             for bits in (32, 64):
                 h = ctypes.c_void_p()
@@ -141,7 +141,7 @@ def test_each_kernel_bank():
                 assert fn("plan_set_kernel_bank", bits)(h, bank) == 0
                 b = ctypes.c_uint()
                 assert fn("plan_get_kernel_bank", bits)(h, ctypes.byref(b)) == 0 and b.value == bank
-                assert fn("plan_set_kernel_bank", bits)(h, 2) == m.Status.INVALID_ARGUMENT
+                assert fn("plan_set_kernel_bank", bits)(h, 4) == m.Status.INVALID_ARGUMENT
                 x = planning_input(TEST_N, bits)
                 y = execute(h, bits, x, False)
                 assert max_abs(y, oracle.dft_ld(x.astype(np.complex128), direction)) <= \
@@ -152,7 +152,7 @@ def test_each_kernel_bank():
 def test_single_stage_radix64_in_place():
     """test_single_stage_in_place (tests/test_planning.c:304-355)."""
     radix = (ctypes.c_int * 1)(64)
-    for bank in (0, 1):
+    for bank in (0, 1, 2, 3):
         for direction in (m.FORWARD, m.BACKWARD):
             for bits in (32, 64):
                 h = ctypes.c_void_p()
@@ -200,7 +200,7 @@ def export(h, bits):
     return raw
 
 
-@pytest.mark.parametrize("bank", [0, 1])
+@pytest.mark.parametrize("bank", [0, 1, 2, 3])
 def test_recipe_replay(bank):
     """check_recipe_case (tests/test_plan_recipe.c:82-191) for n = 64 {4,4,4}
     and 96 {3,4,8}, both directions and placements, both precisions, plus the

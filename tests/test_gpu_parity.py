@@ -125,7 +125,7 @@ def test_two_level_chains_every_radix(radix):
         x = (np.sin(.13 * i) + .01 * (i % 3)) + 1j * (np.cos(.07 * i) - .02 * (i % 5))
         ref = oracle.dft_ld(x, -1)
         for bits, tol in ((32, 64 * FLT_EPS * n), (64, 256 * DBL_EPS * n)):
-            for bank in (0, 1):
+            for bank in (0, 1, 2, 3):
                 y = run_host(x, -1, bits=bits, radices=chain, bank=bank)
                 assert max_abs(y, ref) <= tol, (chain, bits, bank)
                 z = run_host(y, 1, bits=bits, radices=chain, bank=bank) / n
@@ -169,7 +169,7 @@ def test_three_mode_spectral_oracle(n):
     """tests/test_binary_banks.c: the analytic three-mode spectrum, every
     kernel bank, both signs and placements, tolerance 5e-5 / 2e-11."""
     x = three_mode_input(n)
-    for bank in (0, 1):
+    for bank in (0, 1, 2, 3):
         for sign in (-1, 1):
             want = three_mode_expected(n, sign)
             for inplace in (False, True):
@@ -186,7 +186,7 @@ def test_three_mode_single_and_double_radix(radix):
         x = three_mode_input(n)
         for sign in (-1, 1):
             want = three_mode_expected(n, sign)
-            for bank in (0, 1):
+            for bank in (0, 1, 2, 3):
                 for bits, tol in ((32, 5e-5), (64, 2e-11)):
                     y = run_host(x, sign, bits=bits, radices=chain, bank=bank) / n
                     assert max_abs(y, want) <= tol, (chain, sign, bank, bits)

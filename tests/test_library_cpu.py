@@ -151,7 +151,7 @@ def test_recipe_status_per_malformed_field():
         (f"{head} 0a000094 f32 6x -1 0 0 0000000000000000 1 0 3 4 4 4", INV),  # length digit
         (f"{head} 0a000094 f32 64 2 0 0 0000000000000000 1 0 3 4 4 4", INV),  # direction
         (f"{head} 0a000094 f32 64 -1 2 0 0000000000000000 1 0 3 4 4 4", INV),  # placement
-        (f"{head} 0a000094 f32 64 -1 0 2 0000000000000000 1 0 3 4 4 4", INV),  # bank
+        (f"{head} 0a000094 f32 64 -1 0 4 0000000000000000 1 0 3 4 4 4", INV),  # bank
         (f"{head} 0a000094 f32 64 -1 0 0 0000000000000004 1 0 3 4 4 4", INV),  # mask bit
         (f"{head} 0a000094 f32 64 -1 0 0 0000000000000000 2 0 3 4 4 4", INV),  # direct input
         (f"{head} 0a000094 f32 64 -1 0 0 0000000000000000 1 2 3 4 4 4", INV),  # layout
@@ -229,8 +229,13 @@ def test_cost_model_reference_accounting():
 def test_kernel_registry_is_consistent():
     ks = m.kernels()
     generic = [k for k in ks if k["kind"] == m.KERNEL_GENERIC]
-    assert sorted((k["precision_bits"], k["max_radix"]) for k in generic) == \
+    assert sorted(set((k["precision_bits"], k["max_radix"]) for k in generic)) == \
         [(32, 16), (32, 64), (64, 16), (64, 64)]
+    # one runtime-stage kernel per precision, width and kernel bank (0
+    # default codelets; 1-3 like-terms, even-odd, vector-reuse families)
+    assert sorted(k["name"] for k in generic) == sorted(
+        f"generic_{t}{w}{f}" for t in ("float", "double") for w in ("", "_wide")
+        for f in ("", "_lt", "_eo", "_vr"))
     for k in ks:
         if k["kind"] == m.KERNEL_GENERIC:
             continue
@@ -386,3 +391,8 @@ def test_explicit_radices_are_honoured():
     g = m.schedule_preview(4096, 32, bank=1)
     ks = {k["index"]: k for k in m.kernels()}
     assert all(ks[k]["kind"] == m.KERNEL_GENERIC for k in g["kernels"])
+    for bank, suffix in ((1, "_lt"), (2, "_eo"), (3, "_vr")):
+        g = m.schedule_preview(96, 64, bank=bank)
+        assert [ks[k]["name"] for k in g["kernels"]] == [f"generic_double{suffix}"], bank
+    with pytest.raises(m.MofftError):
+        m.schedule_preview(96, 64, bank=4)
