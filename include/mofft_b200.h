@@ -88,6 +88,16 @@ mofft_status mofft_schedule_preview(int precision_bits, size_t length,
                                     mofft_plan_schedule *schedule,
                                     int *chain_out, size_t *chain_count);
 
+/* Device-time model of the schedule that runs `kernels` (registry indices,
+ * one per pass, first pass first) over `batch` transforms of `length`, in
+ * seconds, computed on the host without a GPU; DBL_MAX when the kernels do
+ * not form a schedule of that length.  The planner's prior, as the
+ * reference's cost model is (src/mofft.c:327-351 ranks factorizations,
+ * :874-922 shortlists MEASURE candidates): PRETUNED plans pick among the
+ * splits of their pass count by it, MEASURE times candidates in its order. */
+double mofft_schedule_model_seconds(int precision_bits, size_t length, size_t batch,
+                                    const int *kernels, size_t pass_count);
+
 /* Ragged batches (no counterpart in the reference): many FP32 transforms of
  * different lengths, batch sizes and directions executed by ONE persistent
  * kernel launch over a work-descriptor queue, replayed from a CUDA graph.

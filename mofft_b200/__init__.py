@@ -206,6 +206,7 @@ _PLAIN = [
     ("mofft_schedule_preview", _I, [_I, _SZ, ctypes.POINTER(_I), _SZ, ctypes.c_uint,
                                     ctypes.POINTER(Schedule), ctypes.POINTER(_I),
                                     ctypes.POINTER(_SZ)]),
+    ("mofft_schedule_model_seconds", ctypes.c_double, [_I, _SZ, _SZ, ctypes.POINTER(_I), _SZ]),
 ]
 
 
@@ -290,6 +291,14 @@ def schedule_preview(length: int, bits: int = 32, radices: Optional[Sequence[int
     n = s.pass_count
     return {"pass_count": n, "lengths": list(s.lengths[:n]), "kernels": list(s.kernels[:n]),
             "smem_bytes": list(s.smem_bytes[:n]), "radices": list(chain[: count.value])}
+
+
+def model_seconds(length: int, kernels: Sequence[int], bits: int = 32, batch: int = 1) -> float:
+    """Device-time model of the schedule running `kernels` (one registry index
+    per pass) over `batch` transforms; inf when they do not form one."""
+    arr = _int_array(kernels)
+    t = load().mofft_schedule_model_seconds(bits, length, batch, arr, len(kernels))
+    return float("inf") if t >= 1e300 else float(t)
 
 
 def _int_array(values: Sequence[int]):

@@ -64,6 +64,11 @@ int mofft_ceil_log2_u64(uint64_t x);
 /* Adds n to the process-wide libmofft launch counter. */
 void mofft_count_launches(uint64_t n);
 
+/* Device-time model of a schedule over `batch` transforms (mofft_gpu_model.c),
+ * seconds; DBL_MAX for a schedule it cannot price. */
+double mofft_gpu_schedule_seconds(int precision_bits, size_t length, size_t batch,
+                                  const mofft_schedule *s);
+
 /* MEASURE planner (mofft_measure.c). */
 mofft_status mofft_search_best(mofft_core **out, int precision_bits,
                                size_t length, size_t batch, size_t distance,
