@@ -88,6 +88,24 @@ mofft_status mofft_schedule_preview(int precision_bits, size_t length,
                                     mofft_plan_schedule *schedule,
                                     int *chain_out, size_t *chain_count);
 
+/* How the MEASURE planner's model order compared with its timings (no
+ * counterpart in the reference, whose diagnostics report only the winner):
+ * the number of schedules timed, the model rank of the fastest one (1 = the
+ * model's first choice was fastest), the measured rank of the model's first
+ * choice, the winner's median time and the model's prediction for it.
+ * MOFFT_INVALID_ARGUMENT for a plan that was not measured. */
+typedef struct {
+  size_t candidates;
+  size_t winner_model_rank;
+  size_t model_first_measured_rank;
+  double winner_seconds;
+  double winner_model_seconds;
+} mofft_measure_report;
+mofft_status mofft_plan_get_measure_report_f32(const mofft_plan_f32 *plan,
+                                               mofft_measure_report *report);
+mofft_status mofft_plan_get_measure_report_f64(const mofft_plan_f64 *plan,
+                                               mofft_measure_report *report);
+
 /* Device-time model of the schedule that runs `kernels` (registry indices,
  * one per pass, first pass first) over `batch` transforms of `length`, in
  * seconds, computed on the host without a GPU; DBL_MAX when the kernels do

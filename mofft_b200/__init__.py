@@ -135,8 +135,16 @@ _U64 = ctypes.c_uint64
 
 # (name, restype, argtypes) for every exported entry point; the f32/f64 twins
 # are expanded below.
+class MeasureReport(ctypes.Structure):
+    """mofft_measure_report: the MEASURE planner's model order vs its timings."""
+    _fields_ = [("candidates", ctypes.c_size_t), ("winner_model_rank", ctypes.c_size_t),
+                ("model_first_measured_rank", ctypes.c_size_t),
+                ("winner_seconds", ctypes.c_double), ("winner_model_seconds", ctypes.c_double)]
+
+
 _TYPED = [
     ("mofft_plan_create_{s}", _I, [ctypes.POINTER(_P), _SZ, _I, _I]),
+    ("mofft_plan_get_measure_report_{s}", _I, [_P, ctypes.POINTER(MeasureReport)]),
     ("mofft_plan_create_with_options_{s}", _I,
      [ctypes.POINTER(_P), _SZ, _I, _I, ctypes.POINTER(PlanOptions), ctypes.POINTER(Diagnostics)]),
     ("mofft_plan_dft_1d_{s}", _P, [_SZ, _P, _P, _I, _U32]),
@@ -395,6 +403,12 @@ class Plan:
         prefetching one-pass) recorded a wait that ran out."""
         if self.bits == 32:
             check(self._lib.mofft_plan_check_f32(self._h), "check")
+
+    def measure_report(self) -> dict:
+        """How a MEASURE plan's model order compared with its timings."""
+        r = MeasureReport()
+        check(self._fn("get_measure_report")(self._h, ctypes.byref(r)), "measure report")
+        return {f: getattr(r, f) for f, _ in MeasureReport._fields_}
 
     def schedule(self) -> dict:
         s = Schedule()

@@ -75,6 +75,13 @@ typedef struct mofft_core {
                               pipeline (lazy) */
   size_t stage_bytes;
   pthread_mutex_t lock;
+  /* MEASURE plans: how the model's order compared with the timings */
+  int measured;
+  size_t measure_candidates;
+  size_t measure_winner_model_rank;     /* 1-based, in model order */
+  size_t measure_model_first_rank;      /* measured rank of the model's pick */
+  double measure_winner_seconds;
+  double measure_winner_model_seconds;
 } mofft_core;
 
 struct mofft_plan_f32 { mofft_core core; };

@@ -16,6 +16,7 @@
  * on the plan's stream, and only one candidate's device state is alive at a
  * time besides the shared input/output buffers. */
 #include <cuda_runtime_api.h>
+#include <float.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -28,6 +29,7 @@ typedef struct {
   unsigned bank;
   int preferred[MOFFT_MAX_PASSES];   /* kernel instances to use, -1 = default */
   double model;
+  size_t model_rank;
   double samples[32];
   double median;
 } candidate;
@@ -59,16 +61,16 @@ static void no_preference(candidate *c) {
   for (int i = 0; i < MOFFT_MAX_PASSES; ++i) c->preferred[i] = -1;
 }
 
-/* Model score of a schedule: passes first, then generic kernels. */
-static double model_score(int precision_bits, const candidate *c, size_t length) {
+/* Model score of a schedule: its predicted device seconds over `batch`
+ * transforms (mofft_gpu_model.c), the prior that orders the shortlist. */
+static double model_score(int precision_bits, const candidate *c, size_t length,
+                          size_t batch) {
   mofft_schedule s;
   if (!mofft_group_chain_preferred(precision_bits, c->bank, c->chain, c->count,
                                    (long long)length, c->preferred, &s))
     return INFINITY;
-  double score = 0.0;
-  for (int p = 0; p < s.pass_count; ++p)
-    score += s.pass[p].kind == MOFFT_KERNEL_GENERIC ? 1.6 : 1.0;
-  return score;
+  const double t = mofft_gpu_schedule_seconds(precision_bits, length, batch, &s);
+  return t < DBL_MAX ? t : INFINITY;
 }
 
 static void add_candidate(candidate *pool, int *count, int capacity,
@@ -99,7 +101,7 @@ static int time_compare(const void *l, const void *r) {
 }
 
 /* Every complete schedule the planner can express for this length. */
-static int enumerate(int precision_bits, size_t length, candidate *pool,
+static int enumerate(int precision_bits, size_t length, size_t batch, candidate *pool,
                      int capacity) {
   int count = 0;
   candidate c;
@@ -201,7 +203,7 @@ static int enumerate(int precision_bits, size_t length, candidate *pool,
   c.count = mofft_auto_radices((long long)length, c.chain, MOFFT_MAX_STAGES);
   if (c.count > 0) add_candidate(pool, &count, capacity, &c);
   for (int i = 0; i < count; ++i)
-    pool[i].model = model_score(precision_bits, &pool[i], length);
+    pool[i].model = model_score(precision_bits, &pool[i], length, batch);
   int kept = 0;
   for (int i = 0; i < count; ++i)
     if (isfinite(pool[i].model)) pool[kept++] = pool[i];
@@ -236,10 +238,19 @@ mofft_status mofft_search_best(mofft_core **out, int precision_bits,
   *out = NULL;
   if (length < 2 || !mofft_is_smooth13(length)) return MOFFT_UNSUPPORTED_SIZE;
   if (distance == 0) distance = length;
+  /* Candidates are timed on at most 2^25 points (256 MiB FP32, 512 MiB
+   * FP64 per buffer: larger than L2, so still HBM-bound like the real batch):
+   * the planner's device memory and host input stay bounded however large
+   * the plan's batch is. */
+  size_t mbatch = batch;
+  if (mbatch > 1 && mbatch * distance > ((size_t)1 << 25)) {
+    mbatch = ((size_t)1 << 25) / distance;
+    if (mbatch < 1) mbatch = 1;
+  }
   enum { kPool = 256 };
   candidate *pool = (candidate *)calloc(kPool, sizeof(candidate));
   if (!pool) return MOFFT_ALLOCATION_FAILURE;
-  const int pool_count = enumerate(precision_bits, length, pool, kPool);
+  const int pool_count = enumerate(precision_bits, length, mbatch, pool, kPool);
   if (pool_count == 0) {
     free(pool);
     return MOFFT_UNSUPPORTED_SIZE;
@@ -266,6 +277,14 @@ mofft_status mofft_search_best(mofft_core **out, int precision_bits,
     if (!seen) sel[nsel++] = pool[i];
   }
   free(pool);
+  /* rank of each shortlisted candidate by model seconds (1 = the model's
+   * first choice), recorded before the measurement order is shuffled */
+  for (size_t i = 0; i < nsel; ++i) {
+    size_t rank = 1;
+    for (size_t j = 0; j < nsel; ++j)
+      if (sel[j].model < sel[i].model || (sel[j].model == sel[i].model && j < i)) ++rank;
+    sel[i].model_rank = rank;
+  }
   uint32_t shuffle = (uint32_t)length ^ ((uint32_t)precision_bits << 16) ^
                      UINT32_C(0x9e3779b9);
   for (size_t i = nsel; i > 1; --i) {
@@ -279,7 +298,7 @@ mofft_status mofft_search_best(mofft_core **out, int precision_bits,
   }
 
   const size_t cb = mofft_complex_bytes(precision_bits);
-  const size_t bytes = batch * distance * cb;
+  const size_t bytes = mbatch * distance * cb;
   void *h_in = malloc(bytes);
   void *d_in = NULL, *d_out = NULL, *d_work = NULL;
   cudaEvent_t ev0 = NULL, ev1 = NULL;
@@ -316,11 +335,11 @@ mofft_status mofft_search_best(mofft_core **out, int precision_bits,
     }
   }
   const uint32_t samples = options->timing_samples;
-  const size_t iterations = length * batch < 65536 ? 8 : (length * batch < (1u << 22) ? 4 : 2);
+  const size_t iterations = length * mbatch < 65536 ? 8 : (length * mbatch < (1u << 22) ? 4 : 2);
   for (size_t i = 0; i < nsel; ++i) {
     candidate *cand = &sel[i];
     mofft_core *c = NULL;
-    status = mofft_core_create_tuned(&c, precision_bits, length, batch, distance,
+    status = mofft_core_create_tuned(&c, precision_bits, length, mbatch, distance,
                                      direction, placement, cand->chain, cand->count,
                                      cand->preferred);
     if (status == MOFFT_SUCCESS && cand->bank != 0) {
@@ -379,6 +398,17 @@ mofft_status mofft_search_best(mofft_core **out, int precision_bits,
       mofft_core_destroy(*out);
       *out = NULL;
     }
+  }
+  if (status == MOFFT_SUCCESS) {
+    mofft_core *c = *out;
+    c->measured = 1;
+    c->measure_candidates = nsel;
+    c->measure_winner_model_rank = sel[0].model_rank;
+    c->measure_winner_seconds = sel[0].median;
+    c->measure_winner_model_seconds = sel[0].model;
+    c->measure_model_first_rank = 0;
+    for (size_t i = 0; i < nsel; ++i)
+      if (sel[i].model_rank == 1) c->measure_model_first_rank = i + 1;
   }
   if (status == MOFFT_SUCCESS && diagnostics) {
     diagnostics->measured = 1;

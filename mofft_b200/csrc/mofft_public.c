@@ -548,6 +548,17 @@ static mofft_status create_with_kernels(mofft_core **out, int precision_bits,
     s->workspace_bytes = c->work_bytes;                                          \
     s->twiddle_bytes = c->twiddle_bytes;                                         \
     return MOFFT_SUCCESS;                                                        \
+  }                                                                              \
+  mofft_status mofft_plan_get_measure_report_##SUF(const PLAN *plan,             \
+                                                   mofft_measure_report *r) {    \
+    if (!plan || !r || !plan->core.measured) return MOFFT_INVALID_ARGUMENT;      \
+    const mofft_core *c = CORE(plan);                                            \
+    r->candidates = c->measure_candidates;                                       \
+    r->winner_model_rank = c->measure_winner_model_rank;                         \
+    r->model_first_measured_rank = c->measure_model_first_rank;                  \
+    r->winner_seconds = c->measure_winner_seconds;                               \
+    r->winner_model_seconds = c->measure_winner_model_seconds;                   \
+    return MOFFT_SUCCESS;                                                        \
   }
 
 DEFINE_TYPED_API(f32, 32, mofft_plan_f32, mofft_complex_f32)

@@ -63,11 +63,46 @@ def test_measured_planner():
                 assert d.selected_median_seconds > 0 and d.planning_seconds > 0
                 assert d.length == TEST_N and d.precision_bits == bits
                 assert int(np.prod(d.radix_list())) == TEST_N
+                r = m.MeasureReport()
+                assert fn("plan_get_measure_report", bits)(h, ctypes.byref(r)) == 0
+                assert r.candidates == d.candidates_measured
+                assert 1 <= r.winner_model_rank <= r.candidates
+                assert 1 <= r.model_first_measured_rank <= r.candidates
+                assert r.winner_seconds == d.selected_median_seconds
+                assert r.winner_model_seconds > 0
                 x = planning_input(TEST_N, bits)
                 y = execute(h, bits, x, placement == m.IN_PLACE)
                 ref = oracle.dft_ld(x.astype(np.complex128), direction)
                 assert max_abs(y, ref) <= tol(bits, TEST_N)
                 fn("plan_destroy", bits)(h)
+    # a plan that was not measured has no report
+    with m.Plan.create(64, m.FORWARD, bits=32) as p:
+        with pytest.raises(m.MofftError):
+            p.measure_report()
+
+
+def test_measured_plan_of_a_large_batch():
+    """MEASURE on a batch of 2^26 points (n = 4096 FP32, batch 16384): the
+    candidates are timed on a bounded batch of 2^25 points, the model ranks
+    them first, the report says how the model's order compared, and the plan
+    runs the whole batch correctly."""
+    import torch
+    n, batch = 4096, 16384
+    with m.Plan.create(n, m.FORWARD, m.OUT_OF_PLACE, bits=32, batch=batch,
+                       mode=m.PLANNER_MEASURE, candidate_limit=6, timing_samples=3) as plan:
+        r = plan.measure_report()
+        print("measure report n=4096 batch=16384:", r)
+        assert 1 <= r["winner_model_rank"] <= r["candidates"] <= 6
+        assert r["winner_seconds"] > 0 and r["winner_model_seconds"] > 0
+        x = oracle.uniform(n * batch, seed=3, dtype=np.complex64).reshape(batch, n)
+        d = torch.from_numpy(x).cuda()
+        y = torch.empty_like(d)
+        plan.execute(d, y)
+        torch.cuda.synchronize()
+        rows = [0, 5000, batch - 1]
+        ref = oracle.fft_ld(x[rows].astype(np.complex128), -1)
+        got = y[rows].cpu().numpy()
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 5e-7 * 12
 
 
 def test_large_measured_plan_keeps_input():

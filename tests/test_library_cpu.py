@@ -396,3 +396,45 @@ def test_explicit_radices_are_honoured():
         assert [ks[k]["name"] for k in g["kernels"]] == [f"generic_double{suffix}"], bank
     with pytest.raises(m.MofftError):
         m.schedule_preview(96, 64, bank=4)
+
+
+def _schedule_candidates(n, bits, ks):
+    """The MEASURE planner's candidate shapes: every one-pass kernel of the
+    length, every pair of column kernels, every triple of 64..512-point column
+    kernels (mofft_measure.c, enumerate)."""
+    import itertools
+    out = [[k["index"]] for k in ks if k["kind"] == m.KERNEL_ROWS and
+           k["precision_bits"] == bits and k["length"] == n]
+    cols = [k for k in ks if k["kind"] == m.KERNEL_COLS and k["precision_bits"] == bits]
+    out += [[a["index"], b["index"]] for a, b in itertools.product(cols, cols)
+            if a["length"] * b["length"] == n]
+    narrow = [k for k in cols if 64 <= k["length"] <= 512]
+    out += [[a["index"], b["index"], c["index"]]
+            for a, b, c in itertools.product(narrow, narrow, narrow)
+            if a["length"] * b["length"] * c["length"] == n]
+    return out
+
+
+def test_model_ranks_the_tuned_schedules():
+    """The device-time model is the planner's prior: for most lengths of the
+    compiled wisdom, the schedule the autotuner measured fastest is among the
+    model's two best candidates, and the model's time for it is within a
+    factor of two of the measured one."""
+    import json
+    ks = m.kernels()
+    byname = {k["name"]: k for k in ks}
+    entries = json.loads((ROOT / "mofft_b200" / "wisdom" / "b200_wisdom.json").read_text())
+    top2 = total = 0
+    for e in entries["entries"]:
+        n, bits, batch = e["length"], e["precision_bits"], e["batch"]
+        win = [byname[x]["index"] for x in e["kernels"]]
+        t_win = m.model_seconds(n, win, bits, batch)
+        assert math.isfinite(t_win), e["kernels"]
+        assert 0.5 <= t_win / e["median_seconds"] <= 2.0, (n, bits, t_win, e["median_seconds"])
+        times = [m.model_seconds(n, c, bits, batch) for c in _schedule_candidates(n, bits, ks)]
+        rank = 1 + sum(1 for t in times if math.isfinite(t) and t < t_win * (1 - 1e-9))
+        top2 += rank <= 2
+        total += 1
+    print(f"tuned schedule among the model's two best: {top2}/{total}")
+    assert total >= 90 and top2 >= 0.6 * total
+    assert m.model_seconds(4096, [byname["cols_float_64_t4_c32"]["index"]], 32, 1) == INF
