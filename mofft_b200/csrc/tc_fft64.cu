@@ -327,8 +327,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
       // stage-1 operand: row m = n2 of transform t, K = n1 (re part, then im)
       {
         const float2 *src = a.in + (valid ? b : 0) * a.in_dist + r64;
-        unsigned char *row_hi = a_hi + kmajor_off(m, 0);
-        unsigned char *row_lo = a_lo + kmajor_off(m, 0);
+        // row base (8-row group, row); the swizzled chunk is added per c
+        unsigned char *row_hi = a_hi + (m >> 3) * 1024 + (m & 7) * 128;
+        unsigned char *row_lo = a_lo + (m >> 3) * 1024 + (m & 7) * 128;
 #pragma unroll 2
         for (int c = 0; c < 8; ++c) {
           float re[8], im[8];
