@@ -29,15 +29,20 @@
 // DFT matrix in long double.
 //
 // Work division: one persistent CTA per SM.  Warp 0 allocates TMEM and one of
-// its threads issues every MMA.  Two groups of four warps (warps 4-7, 8-11;
-// each warp reads the TMEM lane quarter of its index mod 4) take turns over
-// pairs of transforms: while one group converts or drains a pair, the tensor
-// core runs the other group's GEMMs.  A group: loads its pair (direct global
-// loads, prefetched into L2 one pair ahead by a bulk prefetch), splits it into
-// its stage-1 operand, waits for stage 1, twiddles and splits the
-// accumulator into its stage-2 operand (same shared buffer), waits for stage
-// 2 and stores the output.  Accumulators of both stages share the group's
-// 128 TMEM columns.
+// its threads issues every MMA; one thread of warp 1 streams the input: each
+// pair of transforms (64 KB) arrives in a shared staging buffer by bulk
+// copies (no multicast) as soon as the previous pair has been read out of
+// it, so HBM reads run while the groups and the tensor core work.  Two
+// groups of eight warps (warps 2-9, 10-17; each warp reads the TMEM lane
+// quarter of its index mod 4, two warps per quarter, each taking half of the
+// quarter's columns) take turns over the CTA's pairs: while one
+// group converts or drains a pair, the tensor core runs the other group's
+// GEMMs.  A group: splits its staged pair into its stage-1 operand, waits
+// for stage 1, twiddles and splits the accumulator into its stage-2 operand
+// (same shared buffer), waits for stage 2 and stores the output.
+// Accumulators of both stages share the group's 128 TMEM columns.  Inputs
+// that are not 16-byte aligned (odd distances) skip the staging: the groups
+// load them from global memory, prefetched into L2 one pair ahead.
 //
 // Every wait (operand ready, MMAs complete) is bounded by one second of
 // wall time.  On a timeout the waiting thread records the error word and
@@ -59,8 +64,10 @@ namespace tc64 {
 
 constexpr int kN = 4096;
 constexpr int kGroups = 2;
-constexpr int kGroupThreads = 128;
-constexpr int kThreads = 128 + kGroups * kGroupThreads;  // warps 0-3, then the groups
+constexpr int kGroupWarps = 8;              // two warps per TMEM lane quarter
+constexpr int kGroupThreads = 32 * kGroupWarps;
+constexpr int kFirstGroupWarp = 2;          // warp 0: MMA issue, warp 1: input stream
+constexpr int kThreads = 32 * kFirstGroupWarp + kGroups * kGroupThreads;
 constexpr int kFormBf16x3 = 2;                            // MOFFT_FORM_BF16X3
 
 // Shared memory (bytes from a 1024-byte aligned base).
@@ -69,9 +76,12 @@ constexpr int kOffB = 0;                    // Fr_hi, Fi_hi, Fr_lo, Fi_lo
 constexpr int kAPart = 128 * 64 * 2;        // M = 128 rows x K = 64 (one part), bf16
 constexpr int kAArray = 2 * kAPart;         // both parts (re, im)
 constexpr int kOffA = 4 * kTile;            // group g: hi at + 2 g kAArray, lo at + kAArray
-constexpr int kOffBar = kOffA + kGroups * 2 * kAArray;
+constexpr int kStage = 2 * kN * 8;         // one pair of transforms, interleaved
+constexpr int kOffS = kOffA + kGroups * 2 * kAArray;   // staging of the next pair
+constexpr int kOffBar = kOffS + kStage;
 constexpr int kOffFlags = kOffBar + 64;     // abort flag, TMEM base
 constexpr int kBytes = kOffFlags + 16 + 1024;
+static_assert(kBytes <= 227 * 1024, "shared memory of the radix-64 kernel");
 constexpr uint32_t kTmemCols = 256;         // group g: D_re at 128 g, D_im at 128 g + 64
 
 // Aux buffer of a plan (global memory): the B tiles as laid out in shared
@@ -175,7 +185,7 @@ struct Args {
   long long in_dist;
   long long out_dist;
   float sign;                 // -1: conjugate on load and store (backward)
-  int prefetch;               // 1: transforms are 16-byte aligned (bulk L2 prefetch)
+  int bulk;                   // 1: transforms are 16-byte aligned (bulk copies)
   int lose_mma;               // failure check: the first GEMM is never issued
 };
 
@@ -226,8 +236,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
   // a_full[g] at bars[g] (128 arrivals), d_full[g] at bars[2 + g] (MMA
-  // commit), fin at bars[4]
+  // commit), fin at bars[4], s_full[g] at bars[5 + g] (staged bytes of
+  // group g's pairs, so that each barrier's phases are one group's pairs in
+  // order), s_empty at bars[7] (128 arrivals of the group that read the
+  // staging buffer)
   const uint32_t bar0 = smem_u32(bars);
+  const uint32_t s_full0 = bar0 + 40, s_empty = bar0 + 56;
 
   for (int i = tid; i < (int)(kAuxTiles / 16); i += kThreads)
     reinterpret_cast<uint4 *>(base + kOffB)[i] = __ldg(reinterpret_cast<const uint4 *>(a.aux) + i);
@@ -239,6 +253,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
                    "r"(1) : "memory");
     }
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0 + 32), "r"(1) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_full0), "r"(1) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_full0 + 8), "r"(1)
+                 : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_empty),
+                 "r"(kGroupThreads) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     *abort_flag = 0;
   }
@@ -294,9 +313,46 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
     // every MMA issued above has completed before TMEM is released
     commit(bar0 + 32);
     (void)line_wait(bar0 + 32, 0);
-  } else if (warp >= 4) {
+  } else if (tid == 32 && a.bulk) {
+    // ------------------------------------------------------------- producer
+    const uint32_t stage_addr = smem_u32(base + kOffS);
+    bool failed = false;
+    long long issued = -1;   // last pair index whose copies were issued
+    for (long long i = 0;; ++i) {
+      const long long pair = blockIdx.x + i * stride;
+      if (pair >= pairs) break;
+      // the group that converted the previous pair has read the buffer
+      if (i > 0 && (*abort_flag || !line_wait(s_empty, (uint32_t)((i - 1) & 1)))) {
+        failed = true;
+        break;
+      }
+      const bool two = 2 * pair + 1 < a.batch;
+      const uint32_t s_full = s_full0 + 8 * (uint32_t)(i & 1);   // group i mod 2
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(s_full),
+                   "r"((two ? 2 : 1) * kN * 8) : "memory");
+      for (int t = 0; t < (two ? 2 : 1); ++t)
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+            "[%3];" ::"r"(stage_addr + (uint32_t)(t * kN * 8)),
+            "l"(a.in + (2 * pair + t) * a.in_dist), "r"(kN * 8), "r"(s_full)
+            : "memory");
+      issued = i;
+    }
+    if (failed) {
+      *abort_flag = 1;
+      atomicExch(a.status, 1);
+    }
+    // the last copy has landed before the shared memory is released
+    if (issued >= 0)
+      (void)line_wait(s_full0 + 8 * (uint32_t)(issued & 1), (uint32_t)((issued >> 1) & 1));
+  } else if (warp >= kFirstGroupWarp) {
     // --------------------------------------------------------------- groups
-    const int g = (warp - 4) >> 2;
+    // Eight warps per group; the two warps of a TMEM lane quarter share its
+    // rows, half h taking half of each row's K chunks (conversion) or
+    // columns (epilogues).
+    const int gw = warp - kFirstGroupWarp;
+    const int g = gw / kGroupWarps;
+    const int h = (gw % kGroupWarps) >> 2;
     const int q = warp & 3;                  // TMEM lane quarter
     const int m = q * 32 + (tid & 31);       // row of both stages' GEMMs
     const int t = m >> 6;                    // transform of the pair
@@ -314,8 +370,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
       if (pair >= pairs) break;
       const long long b = 2 * pair + t;
       const bool valid = b < a.batch;
-      // bulk prefetch of this group's next pair into L2
-      if (a.prefetch && (tid & 127) == 0) {
+      // unaligned inputs: bulk prefetch of this group's next pair into L2
+      if (!a.bulk && gw % kGroupWarps == 0 && (tid & 31) == 0) {
         const long long nb = 2 * (pair + kGroups * stride);
         for (int k = 0; k < 2; ++k)
           if (nb + k < a.batch)
@@ -325,17 +381,25 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
                          : "memory");
       }
       // stage-1 operand: row m = n2 of transform t, K = n1 (re part, then im)
+      if (a.bulk && (*abort_flag || !line_wait(s_full0 + 8 * (uint32_t)g,
+                                                (uint32_t)((i >> 1) & 1)))) {
+        failed = true;
+        break;
+      }
       {
-        const float2 *src = a.in + (valid ? b : 0) * a.in_dist + r64;
+        const float2 *src = a.bulk ? reinterpret_cast<const float2 *>(base + kOffS) +
+                                         t * kN + r64
+                                   : a.in + (valid ? b : 0) * a.in_dist + r64;
         // row base (8-row group, row); the swizzled chunk is added per c
         unsigned char *row_hi = a_hi + (m >> 3) * 1024 + (m & 7) * 128;
         unsigned char *row_lo = a_lo + (m >> 3) * 1024 + (m & 7) * 128;
-#pragma unroll 2
-        for (int c = 0; c < 8; ++c) {
+#pragma unroll
+        for (int c = 4 * h; c < 4 * h + 4; ++c) {
           float re[8], im[8];
 #pragma unroll
           for (int k = 0; k < 8; ++k) {
-            const float2 v = valid ? __ldcg(src + 64 * (8 * c + k)) : make_float2(0.f, 0.f);
+            const float2 v = !valid ? make_float2(0.f, 0.f)
+                             : a.bulk ? src[64 * (8 * c + k)] : __ldcg(src + 64 * (8 * c + k));
             re[k] = v.x;
             im[k] = v.y * a.sign;
           }
@@ -349,6 +413,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
           *reinterpret_cast<uint4 *>(row_lo + kAPart + off) = l;
         }
       }
+      if (a.bulk) arrive(s_empty);   // the staged pair has been read
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       arrive(a_bar);
       if (*abort_flag || !line_wait(d_bar, dphase)) {
@@ -365,7 +430,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
         unsigned char *col_hi = a_hi + kg * 2048 + t * 1024 + kr * 128;
         unsigned char *col_lo = a_lo + kg * 2048 + t * 1024 + kr * 128;
 #pragma unroll 1
-        for (int c2 = 0; c2 < 4; ++c2) {
+        for (int c2 = 2 * h; c2 < 2 * h + 2; ++c2) {
           uint32_t yr[16], yi[16];
           tmem_ld16(trow + 16 * c2, yr);
           tmem_ld16(trow + 64 + 16 * c2, yi);
@@ -405,7 +470,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
       {
         float2 *dst = a.out + (valid ? b : 0) * a.out_dist + r64;
 #pragma unroll 1
-        for (int c2 = 0; c2 < 4; ++c2) {
+        for (int c2 = 2 * h; c2 < 2 * h + 2; ++c2) {
           uint32_t xr[16], xi[16];
           tmem_ld16(trow + 16 * c2, xr);
           tmem_ld16(trow + 64 + 16 * c2, xi);
@@ -456,8 +521,7 @@ struct Inst {
     a.in_dist = p->in_dist;
     a.out_dist = p->out_dist;
     a.sign = p->conj_in ? -1.0f : 1.0f;
-    a.prefetch =
-        ((reinterpret_cast<uintptr_t>(p->in) & 15u) == 0 && (p->in_dist % 2) == 0) ? 1 : 0;
+    a.bulk = ((reinterpret_cast<uintptr_t>(p->in) & 15u) == 0 && (p->in_dist % 2) == 0) ? 1 : 0;
     a.lose_mma = p->lose_copy;
     const long long pairs = (p->batch + 1) / 2;
     const long long grid = pairs < sms ? pairs : sms;   // one CTA per SM
