@@ -176,6 +176,26 @@ __device__ __forceinline__ void split8(const float *v, uint4 &hi, uint4 &lo) {
   lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
+// Bounded wait (one second of %globaltimer, as line_wait) whose polls
+// suspend the waiting thread for up to 20 us each (the try_wait suspend-time
+// hint), so that waiting warps leave the issue slots to the working ones.
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
+  const unsigned long long t0 = line_clock_ns();
+  for (unsigned it = 0; it < (1u << 24); ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity), "r"(20000u)
+        : "memory");
+    if (ok) return true;
+    if (line_clock_ns() - t0 > kLineWaitNs) return false;
+  }
+  return false;
+}
+
 struct Args {
   const float2 *in;
   float2 *out;
@@ -278,32 +298,59 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
 
   if (tid == 0) {
     // ------------------------------------------------------------ MMA issue
-    uint32_t aphase[kGroups] = {0u, 0u};
+    // Serve whichever group's operand is ready (each group's jobs come in
+    // order: stage 1, stage 2 of its pair i, then of pair i + 2), so that one
+    // group's slow phase does not hold the tensor core from the other.
+    uint32_t aphase0 = 0u, aphase1 = 0u;
+    int stage0 = 0, stage1 = 0;
+    long long next0 = 0, next1 = 1;          // CTA-local pair index per group
     const uint32_t b_base = smem_u32(base + kOffB);
     bool lose = a.lose_mma != 0;
     bool failed = false;
-    for (long long i = 0; !failed; i += kGroups) {
-      const long long p0 = blockIdx.x + i * stride;
-      if (p0 >= pairs) break;
-#pragma unroll 1
-      for (int stage = 0; stage < 2 && !failed; ++stage) {
-#pragma unroll 1
-        for (int g = 0; g < kGroups; ++g) {
-          if (blockIdx.x + (i + g) * stride >= pairs) break;
-          if (*abort_flag || !line_wait(bar0 + 8 * g, aphase[g])) {
-            failed = true;
-            break;
-          }
-          aphase[g] ^= 1u;
-          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          if (lose) {  // failure check: this GEMM never runs, its group times out
-            lose = false;
-            continue;
-          }
-          const uint32_t a_hi = smem_u32(base + kOffA + g * 2 * kAArray);
-          issue_stage(tmem + 128u * g, a_hi, a_hi + kAArray, b_base, stage == 1);
-          commit(bar0 + 8 * (2 + g));
+    unsigned long long last = line_clock_ns();
+    for (unsigned spin = 0;; ++spin) {
+      const bool live0 = blockIdx.x + next0 * stride < pairs;
+      const bool live1 = blockIdx.x + next1 * stride < pairs;
+      if (!live0 && !live1) break;
+      bool served = false;
+#pragma unroll
+      for (int g = 0; g < kGroups; ++g) {
+        const bool live = g == 0 ? live0 : live1;
+        const uint32_t ph = g == 0 ? aphase0 : aphase1;
+        if (!live) continue;
+        uint32_t ready;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}"
+            : "=r"(ready)
+            : "r"(bar0 + 8 * g), "r"(ph)
+            : "memory");
+        if (!ready) continue;
+        served = true;
+        const int stage = g == 0 ? stage0 : stage1;
+        if (g == 0) {
+          aphase0 ^= 1u;
+          if (++stage0 == 2) { stage0 = 0; next0 += kGroups; }
+        } else {
+          aphase1 ^= 1u;
+          if (++stage1 == 2) { stage1 = 0; next1 += kGroups; }
         }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (lose) {  // failure check: this GEMM never runs, its group times out
+          lose = false;
+          continue;
+        }
+        const uint32_t a_hi = smem_u32(base + kOffA + g * 2 * kAArray);
+        issue_stage(tmem + 128u * g, a_hi, a_hi + kAArray, b_base, stage == 1);
+        commit(bar0 + 8 * (2 + g));
+      }
+      if (served) {
+        last = line_clock_ns();
+      } else if ((spin & 63u) == 63u &&
+                 (*abort_flag || line_clock_ns() - last > kLineWaitNs)) {
+        failed = true;   // no group became ready for a second, or one gave up
+        break;
       }
     }
     if (failed) {
@@ -312,7 +359,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
     }
     // every MMA issued above has completed before TMEM is released
     commit(bar0 + 32);
-    (void)line_wait(bar0 + 32, 0);
+    (void)bar_wait(bar0 + 32, 0);
   } else if (tid == 32 && a.bulk) {
     // ------------------------------------------------------------- producer
     const uint32_t stage_addr = smem_u32(base + kOffS);
@@ -322,7 +369,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
       const long long pair = blockIdx.x + i * stride;
       if (pair >= pairs) break;
       // the group that converted the previous pair has read the buffer
-      if (i > 0 && (*abort_flag || !line_wait(s_empty, (uint32_t)((i - 1) & 1)))) {
+      if (i > 0 && (*abort_flag || !bar_wait(s_empty, (uint32_t)((i - 1) & 1)))) {
         failed = true;
         break;
       }
@@ -344,7 +391,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
     }
     // the last copy has landed before the shared memory is released
     if (issued >= 0)
-      (void)line_wait(s_full0 + 8 * (uint32_t)(issued & 1), (uint32_t)((issued >> 1) & 1));
+      (void)bar_wait(s_full0 + 8 * (uint32_t)(issued & 1), (uint32_t)((issued >> 1) & 1));
   } else if (warp >= kFirstGroupWarp) {
     // --------------------------------------------------------------- groups
     // Eight warps per group; the two warps of a TMEM lane quarter share its
@@ -362,7 +409,17 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
     const uint32_t a_bar = bar0 + 8 * g;
     const uint32_t d_bar = bar0 + 8 * (2 + g);
     const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + 128u * g;
+    // This thread's twiddles W_4096^(n2 k1) depend only on its fixed n2 and
+    // k1 half: the table entries of W^n2, W^2n2, W^4n2, W^8n2 and of the two
+    // chunk bases W^(16 c2 n2) are read once, and each chunk's sixteen powers
+    // are derived from them (at most three chained products) instead of
+    // loaded per pair (the table does not stay in L1 beside this shared
+    // memory footprint).
     const float2 *tw = reinterpret_cast<const float2 *>(a.aux + kAuxTiles);
+    const float2 p1 = __ldg(tw + 1 * 64 + r64), p2 = __ldg(tw + 2 * 64 + r64);
+    const float2 p4 = __ldg(tw + 4 * 64 + r64), p8 = __ldg(tw + 8 * 64 + r64);
+    const float2 base_lo = __ldg(tw + (32 * h) * 64 + r64);
+    const float2 base_hi = __ldg(tw + (32 * h + 16) * 64 + r64);
     uint32_t dphase = 0;
     bool failed = false;
     for (long long i = g; !failed; i += kGroups) {
@@ -381,7 +438,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
                          : "memory");
       }
       // stage-1 operand: row m = n2 of transform t, K = n1 (re part, then im)
-      if (a.bulk && (*abort_flag || !line_wait(s_full0 + 8 * (uint32_t)g,
+      if (a.bulk && (*abort_flag || !bar_wait(s_full0 + 8 * (uint32_t)g,
                                                 (uint32_t)((i >> 1) & 1)))) {
         failed = true;
         break;
@@ -416,7 +473,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
       if (a.bulk) arrive(s_empty);   // the staged pair has been read
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       arrive(a_bar);
-      if (*abort_flag || !line_wait(d_bar, dphase)) {
+      if (*abort_flag || !bar_wait(d_bar, dphase)) {
         failed = true;
         break;
       }
@@ -436,12 +493,31 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
           tmem_ld16(trow + 64 + 16 * c2, yi);
           tmem_wait_ld();
           float zr[16], zi[16];
+          {
+            // powers W^(n2 k), k < 16, times the chunk base W^(16 c2 n2)
+            float wr[16], wi[16];
+            wr[0] = 1.f; wi[0] = 0.f;
+            wr[1] = p1.x; wi[1] = p1.y;
+            wr[2] = p2.x; wi[2] = p2.y;
+            wr[4] = p4.x; wi[4] = p4.y;
+            wr[8] = p8.x; wi[8] = p8.y;
 #pragma unroll
-          for (int k = 0; k < 16; ++k) {
-            const float2 w = __ldg(tw + (16 * c2 + k) * 64 + r64);
-            const float xr = __uint_as_float(yr[k]), xi = __uint_as_float(yi[k]);
-            zr[k] = xr * w.x - xi * w.y;
-            zi[k] = xr * w.y + xi * w.x;
+            for (int k = 3; k < 16; ++k) {
+              if ((k & (k - 1)) == 0) continue;
+              const int hb = k >= 8 ? 8 : (k >= 4 ? 4 : 2);
+              const int lb = k - hb;
+              wr[k] = wr[hb] * wr[lb] - wi[hb] * wi[lb];
+              wi[k] = wr[hb] * wi[lb] + wi[hb] * wr[lb];
+            }
+            const float2 bs = c2 == 2 * h ? base_lo : base_hi;
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+              const float vr = wr[k] * bs.x - wi[k] * bs.y;
+              const float vi = wr[k] * bs.y + wi[k] * bs.x;
+              const float xr = __uint_as_float(yr[k]), xi = __uint_as_float(yi[k]);
+              zr[k] = xr * vr - xi * vi;
+              zi[k] = xr * vi + xi * vr;
+            }
           }
 #pragma unroll
           for (int h2 = 0; h2 < 2; ++h2) {
@@ -460,7 +536,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       arrive(a_bar);
-      if (*abort_flag || !line_wait(d_bar, dphase)) {
+      if (*abort_flag || !bar_wait(d_bar, dphase)) {
         failed = true;
         break;
       }
