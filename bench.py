@@ -71,6 +71,8 @@ def parse_args():
                    help="requests of the seeded serving stream (bounded sample)")
     p.add_argument("--ragged", action="store_true",
                    help="ragged batch: 512 mixed FP32 transforms, persistent launch vs per item")
+    p.add_argument("--ragged-count", type=int, default=512,
+                   help="items of the ragged batch (a smaller list for profiling)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the C1, precision-form and serving figures of the default run")
@@ -590,7 +592,7 @@ def run_ragged(args, world, rank, local):
     import mofft_b200 as m
     from mofft_b200 import workloads
     torch.cuda.set_device(local)
-    spec = workloads.ragged_spec(count=512, seed=7)
+    spec = workloads.ragged_spec(count=args.ragged_count, seed=7)
     gen = torch.Generator(device="cuda").manual_seed(7)
     items, flops, points = [], 0.0, 0
     for n, batch, direction in spec:
@@ -636,8 +638,8 @@ def run_ragged(args, world, rank, local):
         "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": 3,
         "ms_per_step": round(ragged_ms, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "ragged: 512 transforms, n in {2^6..2^16} U {3*2^5..3*2^13}, "
-                               "batch 1..64, mixed directions, seed 7",
+        "config": {"workload": f"ragged: {args.ragged_count} transforms, n in {{2^6..2^16}} U "
+                               "{3*2^5..3*2^13}, batch 1..64, mixed directions, seed 7",
                    "points": points, "tiles": tiles, "persistent_ctas": grid},
         "per_item_eager": {"ms": round(per_item_ms, 4),
                            "gflops": round(flops / per_item_ms / 1e6, 1)},

@@ -79,39 +79,6 @@ __device__ __forceinline__ void cmul(T& xr, T& xi, T wr, T wi) {
 template <typename T>
 __device__ __forceinline__ cplx_t<T> ld_global(const cplx_t<T>* p) { return __ldcg(p); }
 
-// Strided loads of the column passes: a tile of C adjacent lines reads runs
-// of C elements (32-128 bytes).  MOFFT_COLS_L2_PREFETCH (128 or 256) asks L2
-// to fetch that many bytes around each miss, so that the runs of the tiles
-// next to this one, which run at the same time, find their sectors in L2.
-#ifndef MOFFT_COLS_L2_PREFETCH
-#define MOFFT_COLS_L2_PREFETCH 0
-#endif
-template <typename T>
-__device__ __forceinline__ cplx_t<T> ld_global_strided(const cplx_t<T>* p) {
-#if MOFFT_COLS_L2_PREFETCH == 256 || MOFFT_COLS_L2_PREFETCH == 128
-  cplx_t<T> v;
-  if constexpr (sizeof(T) == 4) {
-#if MOFFT_COLS_L2_PREFETCH == 256
-    asm volatile("ld.global.cg.L2::256B.v2.f32 {%0, %1}, [%2];"
-                 : "=f"(v.x), "=f"(v.y) : "l"(p));
-#else
-    asm volatile("ld.global.cg.L2::128B.v2.f32 {%0, %1}, [%2];"
-                 : "=f"(v.x), "=f"(v.y) : "l"(p));
-#endif
-  } else {
-#if MOFFT_COLS_L2_PREFETCH == 256
-    asm volatile("ld.global.cg.L2::256B.v2.f64 {%0, %1}, [%2];"
-                 : "=d"(v.x), "=d"(v.y) : "l"(p));
-#else
-    asm volatile("ld.global.cg.L2::128B.v2.f64 {%0, %1}, [%2];"
-                 : "=d"(v.x), "=d"(v.y) : "l"(p));
-#endif
-  }
-  return v;
-#else
-  return __ldcg(p);
-#endif
-}
 template <typename T>
 __device__ __forceinline__ void st_global(cplx_t<T>* p, T re, T im) {
   cplx_t<T> v;
@@ -194,7 +161,7 @@ struct ColsLayout {
   __device__ __forceinline__ int saddr(int i) const { return i * PITCH + c; }
   __device__ __forceinline__ void gload(int i, T& re, T& im) const {
     if (active) {
-      const cplx_t<T> v = ld_global_strided<T>(gin + (long long)i * in_stride);
+      const cplx_t<T> v = ld_global<T>(gin + (long long)i * in_stride);
       re = v.x;
       im = v.y * sign_in;
     } else {

@@ -233,7 +233,9 @@ ragged_kernel(const RItem *__restrict__ items, const RTile *__restrict__ tiles,
     const int skip = s_skip;
     if (!skip)
       run_tile(tl.pass == 0 ? itp->cfg0 : itp->cfg1, itp, tl.pass, tl.b, tl.j0, smem);
-    __threadfence();
+    // only a first-pass tile of a two-pass item publishes data that another
+    // CTA reads in this launch: its writes are fenced before the count rises
+    if (tl.pass == 0 && itp->passes == 2) __threadfence();
     __syncthreads();
     if (threadIdx.x == 0 && tl.pass == 0 && itp->passes == 2 && !skip)
       atomicAdd(&done[tl.item], 1);
