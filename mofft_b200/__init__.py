@@ -407,7 +407,7 @@ class Plan:
     def measure_report(self) -> dict:
         """How a MEASURE plan's model order compared with its timings."""
         r = MeasureReport()
-        check(self._fn("get_measure_report")(self._h, ctypes.byref(r)), "measure report")
+        check(self._fn("plan_get_measure_report")(self._h, ctypes.byref(r)), "measure report")
         return {f: getattr(r, f) for f, _ in MeasureReport._fields_}
 
     def schedule(self) -> dict:
