@@ -530,6 +530,13 @@ int mofft_model_chain(int precision_bits, unsigned bank, size_t length,
   collect_divisors(n, 2, 1 << 16, divs, &ndiv, kMaxDiv);
   int best_count = -1;
   group_score best = {1 << 30, 1 << 30, 1e300};
+  double best_seconds = 1e300;
+  /* Splits of the fewest passes are ranked by the device-time model
+   * (mofft_gpu_model.c) over a batch of about 2^25 points, the choice the
+   * reference's choose_factorization makes with its cost model
+   * (src/mofft.c:327-351); a split the model cannot price ranks by the
+   * canonical grouping score. */
+  const size_t model_batch = n >= (1LL << 25) ? 1 : (size_t)((1LL << 25) / n);
   int tmp[MOFFT_MAX_STAGES];
   for (int passes = 2; passes <= 3 && best_count < 0; ++passes) {
     for (int a = 0; a < ndiv; ++a) {
@@ -562,8 +569,19 @@ int mofft_model_chain(int precision_bits, unsigned bank, size_t length,
         if (!try_split(precision_bits, bank, tmp, total_count, cuts, passes, n,
                        NULL, &sched, &score))
           continue;
-        if (best_count < 0 || score_less(&score, &best)) {
+        const double seconds =
+            mofft_gpu_schedule_seconds(precision_bits, (size_t)n, model_batch, &sched);
+        int better;
+        if (best_count < 0 || score.passes != best.passes)
+          better = best_count < 0 || score.passes < best.passes;
+        else if (seconds < 1e300 && best_seconds < 1e300 &&
+                 fabs(seconds - best_seconds) > 1e-3 * best_seconds)
+          better = seconds < best_seconds;
+        else
+          better = score_less(&score, &best);
+        if (better) {
           best = score;
+          best_seconds = seconds;
           best_count = total_count;
           memcpy(chain, tmp, (size_t)total_count * sizeof(int));
         }
