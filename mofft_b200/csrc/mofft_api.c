@@ -612,6 +612,11 @@ void mofft_core_destroy(mofft_core *c) {
   release_device(c);
   if (c->stream) cudaStreamDestroy((cudaStream_t)c->stream);
   if (c->stream2) cudaStreamDestroy((cudaStream_t)c->stream2);
+  if (c->stream3) cudaStreamDestroy((cudaStream_t)c->stream3);
+  for (int i = 0; i < 64; ++i) {
+    if (c->ev_up[i]) cudaEventDestroy((cudaEvent_t)c->ev_up[i]);
+    if (c->ev_done[i]) cudaEventDestroy((cudaEvent_t)c->ev_done[i]);
+  }
   if (saved >= 0 && saved != c->device) cudaSetDevice(saved);
   pthread_mutex_destroy(&c->lock);
   free(c);
@@ -1027,13 +1032,33 @@ static mofft_status enqueue_with_work(const mofft_core *c, const void *in, void 
 
 static mofft_status ensure_staging(mofft_core *c) {
   const size_t bytes = c->batch * c->distance * mofft_complex_bytes(c->precision_bits);
-  if (!c->stream2) {
-    cudaStream_t s2;
-    if (cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking) != cudaSuccess) {
+  if (!c->stream2 || !c->stream3) {
+    cudaStream_t s2 = (cudaStream_t)c->stream2, s3 = (cudaStream_t)c->stream3;
+    if ((!s2 && cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking) != cudaSuccess) ||
+        (!s3 && cudaStreamCreateWithFlags(&s3, cudaStreamNonBlocking) != cudaSuccess)) {
       cudaGetLastError();
       return MOFFT_INTERNAL_ERROR;
     }
     c->stream2 = s2;
+    c->stream3 = s3;
+  }
+  for (int i = 0; i < 64; ++i) {
+    if (!c->ev_up[i]) {
+      cudaEvent_t e;
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return MOFFT_INTERNAL_ERROR;
+      }
+      c->ev_up[i] = e;
+    }
+    if (!c->ev_done[i]) {
+      cudaEvent_t e;
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return MOFFT_INTERNAL_ERROR;
+      }
+      c->ev_done[i] = e;
+    }
   }
   if (c->stage_bytes >= bytes && c->d_stage[0] && c->d_stage[1])
     return MOFFT_SUCCESS;
@@ -1083,9 +1108,11 @@ mofft_status mofft_core_execute(const mofft_core *cc, const void *in, void *out)
     pthread_mutex_lock(&c->lock);
     st = ensure_staging(c);
     if (st == MOFFT_SUCCESS) {
-      /* Chunks of about 24 MiB alternate between two streams, so the upload
-       * of one chunk, the passes of another and the download of a third
-       * overlap (copies from and to pinned memory run on separate engines). */
+      /* Chunks of about 24 MiB flow through three streams: uploads in order
+       * on one, each chunk's passes on another once its upload has landed,
+       * downloads on a third once its passes are done.  Each copy engine
+       * (host to device, device to host) and the SMs then work back to back,
+       * and only real data dependencies (events) order them. */
       const size_t cb = mofft_complex_bytes(c->precision_bits);
       const size_t span = ((c->batch - 1) * c->distance + c->length) * cb;
       const size_t chunk_bytes = (size_t)24 << 20;
@@ -1093,27 +1120,33 @@ mofft_status mofft_core_execute(const mofft_core *cc, const void *in, void *out)
       if (chunks > c->batch) chunks = c->batch;
       if (chunks > 64) chunks = 64;
       if (chunks < 1) chunks = 1;
-      cudaStream_t streams[2] = {(cudaStream_t)c->stream, (cudaStream_t)c->stream2};
+      cudaStream_t up = (cudaStream_t)c->stream2, run = (cudaStream_t)c->stream,
+                   down = (cudaStream_t)c->stream3;
       for (size_t k = 0; k < chunks && st == MOFFT_SUCCESS; ++k) {
         const size_t b0 = k * c->batch / chunks, b1 = (k + 1) * c->batch / chunks;
         if (b1 == b0) continue;
         const size_t off = b0 * c->distance * cb;
         const size_t bytes = ((b1 - b0 - 1) * c->distance + c->length) * cb;
-        cudaStream_t s = streams[k & 1];
         unsigned char *din = (unsigned char *)c->d_stage[0] + off;
         unsigned char *dout = (unsigned char *)c->d_stage[1] + off;
         void *work = c->d_work ? (unsigned char *)c->d_work + b0 * c->length * cb : NULL;
+        cudaEvent_t uploaded = (cudaEvent_t)c->ev_up[k], done = (cudaEvent_t)c->ev_done[k];
         if (cudaMemcpyAsync(din, (const unsigned char *)in + off, bytes,
-                            cudaMemcpyHostToDevice, s) != cudaSuccess)
+                            cudaMemcpyHostToDevice, up) != cudaSuccess ||
+            cudaEventRecord(uploaded, up) != cudaSuccess ||
+            cudaStreamWaitEvent(run, uploaded, 0) != cudaSuccess)
           st = MOFFT_INTERNAL_ERROR;
         if (st == MOFFT_SUCCESS)
-          st = enqueue_with_work(c, din, dout, b1 - b0, c->distance, work, s);
+          st = enqueue_with_work(c, din, dout, b1 - b0, c->distance, work, run);
         if (st == MOFFT_SUCCESS &&
-            cudaMemcpyAsync((unsigned char *)out + off, dout, bytes, cudaMemcpyDeviceToHost,
-                            s) != cudaSuccess)
+            (cudaEventRecord(done, run) != cudaSuccess ||
+             cudaStreamWaitEvent(down, done, 0) != cudaSuccess ||
+             cudaMemcpyAsync((unsigned char *)out + off, dout, bytes, cudaMemcpyDeviceToHost,
+                             down) != cudaSuccess))
           st = MOFFT_INTERNAL_ERROR;
       }
-      for (int i = 0; i < 2; ++i)
+      cudaStream_t streams[3] = {up, run, down};
+      for (int i = 0; i < 3; ++i)
         if (cudaStreamSynchronize(streams[i]) != cudaSuccess && st == MOFFT_SUCCESS)
           st = MOFFT_INTERNAL_ERROR;
       if (st != MOFFT_SUCCESS) cudaGetLastError();

@@ -71,6 +71,9 @@ typedef struct mofft_core {
   void *stream;            /* plan-owned cudaStream_t */
   void *user_stream;       /* attached cudaStream_t, or NULL */
   void *d_stage[2];        /* host-pointer staging buffers (lazy) */
+  void *stream3;           /* download stream of the host-buffer pipeline */
+  void *ev_up[64];         /* per-chunk events: upload done, passes done */
+  void *ev_done[64];
   void *stream2;           /* second plan-owned stream of the host-buffer
                               pipeline (lazy) */
   size_t stage_bytes;
