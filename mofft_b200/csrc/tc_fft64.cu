@@ -63,8 +63,14 @@ namespace mofft {
 namespace tc64 {
 
 constexpr int kN = 4096;
-constexpr int kGroups = 2;
-constexpr int kGroupWarps = 8;              // two warps per TMEM lane quarter
+#ifndef MOFFT_TC64_GROUPS
+#define MOFFT_TC64_GROUPS 2
+#endif
+constexpr int kGroups = MOFFT_TC64_GROUPS;
+// two groups of eight warps with an input staging buffer, or three groups of
+// four warps (their operands take the staging buffer's shared memory)
+constexpr bool kStaging = kGroups == 2;
+constexpr int kGroupWarps = kGroups == 2 ? 8 : 4;
 constexpr int kGroupThreads = 32 * kGroupWarps;
 constexpr int kFirstGroupWarp = 2;          // warp 0: MMA issue, warp 1: input stream
 constexpr int kThreads = 32 * kFirstGroupWarp + kGroups * kGroupThreads;
@@ -78,11 +84,11 @@ constexpr int kAArray = 2 * kAPart;         // both parts (re, im)
 constexpr int kOffA = 4 * kTile;            // group g: hi at + 2 g kAArray, lo at + kAArray
 constexpr int kStage = 2 * kN * 8;         // one pair of transforms, interleaved
 constexpr int kOffS = kOffA + kGroups * 2 * kAArray;   // staging of the next pair
-constexpr int kOffBar = kOffS + kStage;
-constexpr int kOffFlags = kOffBar + 64;     // abort flag, TMEM base
+constexpr int kOffBar = kOffS + (kStaging ? kStage : 0);
+constexpr int kOffFlags = kOffBar + 128;    // abort flag, TMEM base
 constexpr int kBytes = kOffFlags + 16 + 1024;
 static_assert(kBytes <= 227 * 1024, "shared memory of the radix-64 kernel");
-constexpr uint32_t kTmemCols = 256;         // group g: D_re at 128 g, D_im at 128 g + 64
+constexpr uint32_t kTmemCols = kGroups == 2 ? 256 : 512;  // group g: D_re at 128 g, D_im + 64
 
 // Aux buffer of a plan (global memory): the B tiles as laid out in shared
 // memory, then the twiddle table W_4096^(k1 n2) at [k1][n2].
@@ -255,13 +261,14 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(base + kOffFlags + 4);
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
-  // a_full[g] at bars[g] (128 arrivals), d_full[g] at bars[2 + g] (MMA
-  // commit), fin at bars[4], s_full[g] at bars[5 + g] (staged bytes of
-  // group g's pairs, so that each barrier's phases are one group's pairs in
-  // order), s_empty at bars[7] (128 arrivals of the group that read the
-  // staging buffer)
+  // a_full[g] at bars[g] (a group's arrivals), d_full[g] at
+  // bars[kGroups + g] (MMA commit), fin at bars[2 kGroups], s_full[g] at
+  // bars[2 kGroups + 1 + g] (staged bytes of group g's pairs, so that each
+  // barrier's phases are one group's pairs in order), s_empty after them
+  // (arrivals of the group that read the staging buffer)
   const uint32_t bar0 = smem_u32(bars);
-  const uint32_t s_full0 = bar0 + 40, s_empty = bar0 + 56;
+  const uint32_t d_full0 = bar0 + 8 * kGroups, fin = bar0 + 16 * kGroups;
+  const uint32_t s_full0 = fin + 8, s_empty = fin + 24;
 
   for (int i = tid; i < (int)(kAuxTiles / 16); i += kThreads)
     reinterpret_cast<uint4 *>(base + kOffB)[i] = __ldg(reinterpret_cast<const uint4 *>(a.aux) + i);
@@ -269,10 +276,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
     for (int g = 0; g < kGroups; ++g) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0 + 8 * g),
                    "r"(kGroupThreads) : "memory");
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0 + 8 * (2 + g)),
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(d_full0 + 8 * g),
                    "r"(1) : "memory");
     }
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0 + 32), "r"(1) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(fin), "r"(1) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_full0), "r"(1) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_full0 + 8), "r"(1)
                  : "memory");
@@ -299,42 +306,42 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
   if (tid == 0) {
     // ------------------------------------------------------------ MMA issue
     // Serve whichever group's operand is ready (each group's jobs come in
-    // order: stage 1, stage 2 of its pair i, then of pair i + 2), so that one
-    // group's slow phase does not hold the tensor core from the other.
-    uint32_t aphase0 = 0u, aphase1 = 0u;
-    int stage0 = 0, stage1 = 0;
-    long long next0 = 0, next1 = 1;          // CTA-local pair index per group
+    // order: stage 1, stage 2 of its pair i, then of pair i + kGroups), so
+    // that one group's slow phase does not hold the tensor core from another.
+    uint32_t aphase[kGroups];
+    int stg[kGroups];
+    long long nxt[kGroups];                  // CTA-local pair index per group
+#pragma unroll
+    for (int g = 0; g < kGroups; ++g) {
+      aphase[g] = 0u;
+      stg[g] = 0;
+      nxt[g] = g;
+    }
     const uint32_t b_base = smem_u32(base + kOffB);
     bool lose = a.lose_mma != 0;
     bool failed = false;
     unsigned long long last = line_clock_ns();
     for (unsigned spin = 0;; ++spin) {
-      const bool live0 = blockIdx.x + next0 * stride < pairs;
-      const bool live1 = blockIdx.x + next1 * stride < pairs;
-      if (!live0 && !live1) break;
-      bool served = false;
+      bool any = false, served = false;
 #pragma unroll
       for (int g = 0; g < kGroups; ++g) {
-        const bool live = g == 0 ? live0 : live1;
-        const uint32_t ph = g == 0 ? aphase0 : aphase1;
-        if (!live) continue;
+        if (blockIdx.x + nxt[g] * stride >= pairs) continue;
+        any = true;
         uint32_t ready;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
             "selp.b32 %0, 1, 0, p;\n\t}"
             : "=r"(ready)
-            : "r"(bar0 + 8 * g), "r"(ph)
+            : "r"(bar0 + 8 * g), "r"(aphase[g])
             : "memory");
         if (!ready) continue;
         served = true;
-        const int stage = g == 0 ? stage0 : stage1;
-        if (g == 0) {
-          aphase0 ^= 1u;
-          if (++stage0 == 2) { stage0 = 0; next0 += kGroups; }
-        } else {
-          aphase1 ^= 1u;
-          if (++stage1 == 2) { stage1 = 0; next1 += kGroups; }
+        const int stage = stg[g];
+        aphase[g] ^= 1u;
+        if (++stg[g] == 2) {
+          stg[g] = 0;
+          nxt[g] += kGroups;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         if (lose) {  // failure check: this GEMM never runs, its group times out
@@ -343,8 +350,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
         }
         const uint32_t a_hi = smem_u32(base + kOffA + g * 2 * kAArray);
         issue_stage(tmem + 128u * g, a_hi, a_hi + kAArray, b_base, stage == 1);
-        commit(bar0 + 8 * (2 + g));
+        commit(d_full0 + 8 * g);
       }
+      if (!any) break;
       if (served) {
         last = line_clock_ns();
       } else if ((spin & 63u) == 63u &&
@@ -358,9 +366,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
       atomicExch(a.status, 1);
     }
     // every MMA issued above has completed before TMEM is released
-    commit(bar0 + 32);
-    (void)bar_wait(bar0 + 32, 0);
-  } else if (tid == 32 && a.bulk) {
+    commit(fin);
+    (void)bar_wait(fin, 0);
+  } else if (kStaging && tid == 32 && a.bulk) {
     // ------------------------------------------------------------- producer
     const uint32_t stage_addr = smem_u32(base + kOffS);
     bool failed = false;
@@ -399,7 +407,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
     // columns (epilogues).
     const int gw = warp - kFirstGroupWarp;
     const int g = gw / kGroupWarps;
-    const int h = (gw % kGroupWarps) >> 2;
+    const int h = kGroupWarps == 8 ? (gw % kGroupWarps) >> 2 : 0;
     const int q = warp & 3;                  // TMEM lane quarter
     const int m = q * 32 + (tid & 31);       // row of both stages' GEMMs
     const int t = m >> 6;                    // transform of the pair
@@ -407,7 +415,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
     unsigned char *a_hi = base + kOffA + g * 2 * kAArray;
     unsigned char *a_lo = a_hi + kAArray;
     const uint32_t a_bar = bar0 + 8 * g;
-    const uint32_t d_bar = bar0 + 8 * (2 + g);
+    const uint32_t d_bar = d_full0 + 8 * g;
     const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + 128u * g;
     // This thread's twiddles W_4096^(n2 k1) depend only on its fixed n2 and
     // k1 half: the table entries of W^n2, W^2n2, W^4n2, W^8n2 and of the two
@@ -418,8 +426,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
     const float2 *tw = reinterpret_cast<const float2 *>(a.aux + kAuxTiles);
     const float2 p1 = __ldg(tw + 1 * 64 + r64), p2 = __ldg(tw + 2 * 64 + r64);
     const float2 p4 = __ldg(tw + 4 * 64 + r64), p8 = __ldg(tw + 8 * 64 + r64);
-    const float2 base_lo = __ldg(tw + (32 * h) * 64 + r64);
-    const float2 base_hi = __ldg(tw + (32 * h + 16) * 64 + r64);
+    constexpr int kChunks = 4 * 4 / kGroupWarps;   // 16-column chunks per thread
+    const int c2_first = kChunks * h;
+    float2 base_c2[kChunks];                       // W^(16 c2 n2) of each chunk
+#pragma unroll
+    for (int j = 0; j < kChunks; ++j) base_c2[j] = __ldg(tw + (16 * (c2_first + j)) * 64 + r64);
     uint32_t dphase = 0;
     bool failed = false;
     for (long long i = g; !failed; i += kGroups) {
@@ -451,7 +462,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
         unsigned char *row_hi = a_hi + (m >> 3) * 1024 + (m & 7) * 128;
         unsigned char *row_lo = a_lo + (m >> 3) * 1024 + (m & 7) * 128;
 #pragma unroll
-        for (int c = 4 * h; c < 4 * h + 4; ++c) {
+        for (int c = 2 * kChunks * h; c < 2 * kChunks * (h + 1); ++c) {
           float re[8], im[8];
 #pragma unroll
           for (int k = 0; k < 8; ++k) {
@@ -487,7 +498,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
         unsigned char *col_hi = a_hi + kg * 2048 + t * 1024 + kr * 128;
         unsigned char *col_lo = a_lo + kg * 2048 + t * 1024 + kr * 128;
 #pragma unroll 1
-        for (int c2 = 2 * h; c2 < 2 * h + 2; ++c2) {
+        for (int c2 = c2_first; c2 < c2_first + kChunks; ++c2) {
           uint32_t yr[16], yi[16];
           tmem_ld16(trow + 16 * c2, yr);
           tmem_ld16(trow + 64 + 16 * c2, yi);
@@ -509,7 +520,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
               wr[k] = wr[hb] * wr[lb] - wi[hb] * wi[lb];
               wi[k] = wr[hb] * wi[lb] + wi[hb] * wr[lb];
             }
-            const float2 bs = c2 == 2 * h ? base_lo : base_hi;
+            float2 bs = base_c2[0];
+#pragma unroll
+            for (int j = 1; j < kChunks; ++j)
+              if (c2 == c2_first + j) bs = base_c2[j];
 #pragma unroll
             for (int k = 0; k < 16; ++k) {
               const float vr = wr[k] * bs.x - wi[k] * bs.y;
@@ -546,7 +560,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc64_fft4096_kernel(const Args a)
       {
         float2 *dst = a.out + (valid ? b : 0) * a.out_dist + r64;
 #pragma unroll 1
-        for (int c2 = 2 * h; c2 < 2 * h + 2; ++c2) {
+        for (int c2 = c2_first; c2 < c2_first + kChunks; ++c2) {
           uint32_t xr[16], xi[16];
           tmem_ld16(trow + 16 * c2, xr);
           tmem_ld16(trow + 64 + 16 * c2, xi);
@@ -597,7 +611,8 @@ struct Inst {
     a.in_dist = p->in_dist;
     a.out_dist = p->out_dist;
     a.sign = p->conj_in ? -1.0f : 1.0f;
-    a.bulk = ((reinterpret_cast<uintptr_t>(p->in) & 15u) == 0 && (p->in_dist % 2) == 0) ? 1 : 0;
+    a.bulk = (kStaging && (reinterpret_cast<uintptr_t>(p->in) & 15u) == 0 &&
+              (p->in_dist % 2) == 0) ? 1 : 0;
     a.lose_mma = p->lose_copy;
     const long long pairs = (p->batch + 1) / 2;
     const long long grid = pairs < sms ? pairs : sms;   // one CTA per SM
