@@ -16,6 +16,10 @@ const Entry *entries_cols_f32(int *count) {
       COLS(float, 1024, 32, 16, 16, 16, 4),
       COLS(float, 2048, 128, 8, 16, 16, 8),
       COLS(float, 4096, 256, 4, 16, 16, 16),
+      COLS(float, 64, 4, 64, 16, 4),
+      COLS(float, 128, 8, 32, 16, 8),
+      COLS(float, 512, 32, 8, 16, 16, 2),
+      COLS(float, 1024, 64, 4, 16, 16, 4),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;
