@@ -228,9 +228,9 @@ mofft_status mofft_plan_get_precision_form_f32(const mofft_plan_f32 *plan,
                                                mofft_precision_form *form);
 /* Synchronizes the plan's stream and reports MOFFT_INTERNAL_ERROR when a
  * kernel of the plan that bounds its waits (the tensor-core kernels, the
- * prefetching one-pass kernel rows_float_16384_t512_b1_sfalse_dxp) recorded a
- * wait that ran out.  Blocking executes without an attached stream check
- * this themselves. */
+ * prefetching one-pass kernel rows_float_16384_t512_b1_sfalse_dxp, the
+ * thread-block-cluster kernels cluster_*) recorded a wait that ran out.
+ * Blocking executes without an attached stream check this themselves. */
 mofft_status mofft_plan_check_f32(mofft_plan_f32 *plan);
 /* Failure check of a one-pass plan whose kernel bulk-copies its input: one
  * forward launch on device buffers `input` / `output` in which the first
@@ -238,7 +238,9 @@ mofft_status mofft_plan_check_f32(mofft_plan_f32 *plan);
  * out (about a second).  The tensor-core n = 4096 kernel then frees its
  * tensor memory and returns, leaving `output` unspecified; the prefetching
  * one-pass kernel loads those lines itself, so `output` is still the forward
- * transform.  Returns the status an execute would then report --
+ * transform; in a cluster kernel CTA 0 of every cluster never sends its
+ * tiles, so every CTA's wait for its tiles runs out and `output` is
+ * unspecified.  Returns the status an execute would then report --
  * MOFFT_INTERNAL_ERROR when the timeout path works -- and clears the plan's
  * error word, so the plan stays usable.  MOFFT_INVALID_ARGUMENT for plans
  * that run neither kernel.  For tests of the timeout path. */

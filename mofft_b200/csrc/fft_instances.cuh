@@ -284,5 +284,6 @@ const Entry *entries_rows_mixed(int *count);
 const Entry *entries_cols_mixed(int *count);
 const Entry *entries_tensor(int *count);
 const Entry *entries_tensor64(int *count);
+const Entry *entries_cluster(int *count);
 
 }  // namespace mofft

@@ -17,7 +17,7 @@ const std::vector<Entry> &registry() {
                                       entries_rows_f64, entries_cols_f32,
                                       entries_cols_f64, entries_rows_mixed,
                                       entries_cols_mixed, entries_tensor64,
-                                      entries_tensor};
+                                      entries_tensor, entries_cluster};
     for (auto list : lists) {
       int n = 0;
       const Entry *e = list(&n);

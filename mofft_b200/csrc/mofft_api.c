@@ -238,7 +238,9 @@ static int chain_equal(const int *a, int na, const int *b, int nb) {
   return 1;
 }
 
-/* Specialised kernel whose in-CTA chain equals `chain`. */
+/* Specialised kernel whose in-CTA chain equals `chain`.  The thread-block
+ * cluster kernels are never found here: they run when a tuned or explicit
+ * kernel list names them (MEASURE times them against the others). */
 static int find_special(int precision_bits, int kind, const int *chain,
                         int count, long long total, long long ns_outer) {
   long long length = 1;
@@ -247,7 +249,7 @@ static int find_special(int precision_bits, int kind, const int *chain,
   for (int i = 0; i < n; ++i) {
     const mofft_kernel_desc *d = mofft_cuda_kernel_get(i);
     if (d->kind != kind || d->precision_bits != precision_bits ||
-        d->length != length ||
+        d->length != length || d->cluster > 0 ||
         !chain_equal(d->radices, d->radix_count, chain, count))
       continue;
     if (kind == MOFFT_KERNEL_COLS) {
@@ -485,7 +487,7 @@ static int preferred_chain(int precision_bits, unsigned bank, int kind,
     for (int i = 0; i < n; ++i) {
       const mofft_kernel_desc *d = mofft_cuda_kernel_get(i);
       if (d->kind != kind || d->precision_bits != precision_bits ||
-          d->length != length || d->radix_count > capacity)
+          d->length != length || d->radix_count > capacity || d->cluster > 0)
         continue;
       if (kind == MOFFT_KERNEL_COLS) {
         if ((total / length) % d->lines != 0) continue;
@@ -510,14 +512,30 @@ static void collect_divisors(long long n, long long lo, long long hi,
   }
 }
 
+static int model_chain(int precision_bits, unsigned bank, size_t length, int *chain,
+                       int capacity, int one_pass);
+
 /* Analytical PRETUNED chain for a whole transform of `length`. */
 int mofft_model_chain(int precision_bits, unsigned bank, size_t length,
                       int *chain, int capacity) {
+  return model_chain(precision_bits, bank, length, chain, capacity, 1);
+}
+
+/* The best chain of two or more passes (callers that need the intermediate
+ * array of a multi-pass schedule even where one pass exists). */
+int mofft_model_chain_multipass(int precision_bits, unsigned bank, size_t length,
+                                int *chain, int capacity) {
+  return model_chain(precision_bits, bank, length, chain, capacity, 0);
+}
+
+static int model_chain(int precision_bits, unsigned bank, size_t length, int *chain,
+                       int capacity, int one_pass) {
   mofft_schedule sched;
   /* one pass */
-  int count = preferred_chain(precision_bits, bank, MOFFT_KERNEL_ROWS,
-                              (long long)length, (long long)length, 1, chain,
-                              capacity);
+  int count = one_pass ? preferred_chain(precision_bits, bank, MOFFT_KERNEL_ROWS,
+                                         (long long)length, (long long)length, 1, chain,
+                                         capacity)
+                       : 0;
   if (count > 0 && mofft_group_chain(precision_bits, bank, chain, count,
                                      (long long)length, &sched) &&
       sched.pass_count == 1)
@@ -628,12 +646,20 @@ static int is_tensor_kind(int kind) {
   return kind == MOFFT_KERNEL_TENSOR || kind == MOFFT_KERNEL_TENSOR_COLS;
 }
 
+/* Passes that read a constant table next to their twiddles: the tensor-core
+ * kernels (operand tiles) and every kernel that carries a table of its own
+ * (the radix-64 tensor-core kernel, the cluster kernels). */
+static int pass_has_aux(const mofft_pass *ps) {
+  return is_tensor_kind(ps->kind) || mofft_cuda_kernel_aux_bytes(ps->kernel) > 0;
+}
+
 /* Passes whose kernel reports bounded-wait timeouts in an error word: the
- * tensor-core kernels and the prefetching ROWS kernels. */
+ * tensor-core kernels, the prefetching ROWS kernels and the cluster kernels
+ * (their wait for the exchanged tiles). */
 static int pass_has_status(const mofft_pass *ps) {
   if (is_tensor_kind(ps->kind)) return 1;
   const mofft_kernel_desc *d = mofft_cuda_kernel_get(ps->kernel);
-  return ps->kind == MOFFT_KERNEL_ROWS && d && d->prefetch;
+  return ps->kind == MOFFT_KERNEL_ROWS && d && (d->prefetch || d->cluster > 0);
 }
 
 static int schedule_has_status(const mofft_core *c) {
@@ -664,7 +690,7 @@ static mofft_status materialise_schedule(mofft_core *c) {
       bytes = align256(bytes + lo_n * cb);
     }
     ps->aux_offset = ps->status_offset = 0;
-    if (is_tensor_kind(ps->kind)) {
+    if (pass_has_aux(ps)) {
       ps->aux_offset = bytes;
       const size_t own = mofft_cuda_kernel_aux_bytes(ps->kernel);
       bytes = align256(bytes + (own ? own
@@ -690,7 +716,7 @@ static mofft_status materialise_schedule(mofft_core *c) {
       mofft_write_twiddles(host + ps->tw_hi_offset, c->precision_bits, m, 0, lo_n, hi_n);
       mofft_write_twiddles(host + ps->tw_lo_offset, c->precision_bits, m, 0, 1, lo_n);
     }
-    if (is_tensor_kind(ps->kind) && mofft_cuda_kernel_aux_bytes(ps->kernel)) {
+    if (mofft_cuda_kernel_aux_bytes(ps->kernel)) {
       if (mofft_cuda_kernel_fill_aux(ps->kernel, host + ps->aux_offset) != 0) {
         free(host);
         return MOFFT_INTERNAL_ERROR;
@@ -818,7 +844,7 @@ mofft_status mofft_core_check_lost_copy(mofft_core *c, const void *in, void *out
   a.in = in;
   a.out = out;
   a.tw = (const unsigned char *)c->d_twiddles + ps->tw_offset;
-  if (is_tensor_kind(ps->kind)) a.aux = (const unsigned char *)c->d_twiddles + ps->aux_offset;
+  if (pass_has_aux(ps)) a.aux = (const unsigned char *)c->d_twiddles + ps->aux_offset;
   a.status = (int *)((unsigned char *)c->d_twiddles + ps->status_offset);
   a.batch = (long long)c->batch;
   a.in_dist = (long long)c->distance;
@@ -1008,7 +1034,7 @@ static mofft_status enqueue_with_work(const mofft_core *c, const void *in, void 
     a.split_shift = ps->split_shift;
     a.conj_in = backward && p == 0;
     a.conj_out = backward && p == P - 1;
-    if (is_tensor_kind(ps->kind))
+    if (pass_has_aux(ps))
       a.aux = (const unsigned char *)c->d_twiddles + ps->aux_offset;
     if (pass_has_status(ps))
       a.status = (int *)((unsigned char *)c->d_twiddles + ps->status_offset);
@@ -1241,6 +1267,8 @@ mofft_status mofft_core_enqueue_indirect(const mofft_core *c, const void *const 
     a.lines = ps->lines;
     a.radix_count = ps->radix_count;
     memcpy(a.radices, ps->radices, sizeof(a.radices));
+    if (pass_has_aux(ps))
+      a.aux = (const unsigned char *)c->d_twiddles + ps->aux_offset;
     if (pass_has_status(ps))
       a.status = (int *)((unsigned char *)c->d_twiddles + ps->status_offset);
     const int err = mofft_cuda_launch_pass(ps->kernel, &a, stream);

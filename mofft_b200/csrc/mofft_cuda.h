@@ -42,6 +42,8 @@ typedef struct {
   int bank;             /* kernel bank whose codelets it runs: 0 default,
                            1 like-terms, 2 even-odd, 3 vector-reuse families
                            (runtime-stage kernels) */
+  int cluster;          /* ROWS: CTAs of the thread-block cluster that computes
+                           one transform (0: one CTA per transform) */
 } mofft_kernel_desc;
 
 typedef struct {

@@ -27,6 +27,9 @@ int mofft_group_chain_preferred(int precision_bits, unsigned bank,
 int mofft_auto_radices(long long length, int *out, int capacity);
 int mofft_model_chain(int precision_bits, unsigned bank, size_t length,
                       int *chain, int capacity);
+/* The best chain of two or more passes for `length` (-1 if none). */
+int mofft_model_chain_multipass(int precision_bits, unsigned bank, size_t length,
+                                int *chain, int capacity);
 
 mofft_status mofft_core_create(mofft_core **out, int precision_bits,
                                size_t length, size_t batch, size_t distance,

@@ -143,9 +143,17 @@ extern "C" mofft_status mofft_execute_fixed_scratch_f32(
       sched.pass_count = 0;
   }
   if (sched.pass_count != 2) {
-    const int count = mofft_model_chain(32, 0, length, chain, MOFFT_MAX_STAGES);
+    int count = mofft_model_chain(32, 0, length, chain, MOFFT_MAX_STAGES);
     if (count <= 0 || !mofft_group_chain(32, 0, chain, count, (long long)length, &sched))
       return MOFFT_UNSUPPORTED_SIZE;
+    // A length that a thread-block cluster computes in one pass still has its
+    // two-pass schedule here: this entry point is the two-pass path.
+    const mofft_kernel_desc *d = mofft_cuda_kernel_get(sched.pass[0].kernel);
+    if (sched.pass_count == 1 && d && d->cluster > 0) {
+      count = mofft_model_chain_multipass(32, 0, length, chain, MOFFT_MAX_STAGES);
+      if (count <= 0 || !mofft_group_chain(32, 0, chain, count, (long long)length, &sched))
+        return MOFFT_UNSUPPORTED_SIZE;
+    }
   }
   if (sched.pass_count != 2) return MOFFT_UNSUPPORTED_SIZE;
 

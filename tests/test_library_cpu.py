@@ -371,12 +371,18 @@ def test_planner_covers_every_length(bits):
 
 
 def test_planner_power_of_two_pass_counts():
-    """Minimal pass counts of the HBM roofline: P = ceil(log2 n / 14) for
-    FP32 and ceil(log2 n / 13) for FP64, up to 2^24 / 2^22."""
+    """Pass counts of the model's schedules: ceil(log2 n / 14) for FP32 and
+    ceil(log2 n / 13) for FP64, up to 2^24 / 2^22 (one CTA holds 2^14 FP32 /
+    2^13 FP64 points; the thread-block cluster kernels, which hold up to 2^16
+    / 2^15, run only when a tuned or explicit kernel list names them)."""
     for e in range(1, 25):
-        assert m.schedule_preview(2 ** e, 32)["pass_count"] == math.ceil(e / 14)
+        assert m.schedule_preview(2 ** e, 32)["pass_count"] == math.ceil(e / 14), e
     for e in range(1, 23):
-        assert m.schedule_preview(2 ** e, 64)["pass_count"] == math.ceil(e / 13)
+        assert m.schedule_preview(2 ** e, 64)["pass_count"] == math.ceil(e / 13), e
+    ks = {k["index"]: k for k in m.kernels()}
+    for n, bits in ((16384, 32), (32768, 32), (65536, 32), (16384, 64), (32768, 64)):
+        s = m.schedule_preview(n, bits)
+        assert not any(ks[k]["name"].startswith("cluster_") for k in s["kernels"]), (n, bits)
 
 
 def test_explicit_radices_are_honoured():
