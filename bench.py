@@ -584,9 +584,11 @@ def run_sweep(args, world, rank, local):
 
 
 def run_ragged(args, world, rank, local):
-    """512 FP32 transforms of mixed length / batch / direction (seed 7): one
-    persistent launch from a CUDA graph vs one plain launch per transform
-    (eager, and captured in a CUDA graph)."""
+    """512 FP32 transforms of mixed length / batch / direction (seed 7): the
+    ragged plan's CUDA graph (one persistent launch for the one-pass lengths,
+    tuned groups for the longer ones) vs every item in the persistent launch
+    vs one plain launch per transform (eager, and captured in a CUDA
+    graph)."""
     import torch
 
     import mofft_b200 as m
@@ -619,6 +621,12 @@ def run_ragged(args, world, rank, local):
 
     ragged_ms = timed(lambda: plan.execute(sh), args.steps)
     assert plan.status() == 0, "ragged kernel reported a timed-out dependency wait"
+    single = m.RaggedPlan(items, single_launch=True)
+    single_ms = timed(lambda: single.execute(sh), args.steps)
+    assert single.status() == 0, "ragged kernel reported a timed-out dependency wait"
+    single.destroy()
+    # minimal-pass bytes: P(n) reads and writes of every point
+    min_bytes = sum(n * batch * 16 * passes_for(n, 32) for n, batch, _ in spec)
     per_item_ms = timed(lambda: plan.execute_per_item(sh), max(3, args.steps // 4))
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.stream(stream):
@@ -644,8 +652,11 @@ def run_ragged(args, world, rank, local):
         "per_item_eager": {"ms": round(per_item_ms, 4),
                            "gflops": round(flops / per_item_ms / 1e6, 1)},
         "per_item_graph": {"ms": round(graph_ms, 4), "gflops": round(flops / graph_ms / 1e6, 1)},
+        "single_launch": {"ms": round(single_ms, 4),
+                          "gflops": round(flops / single_ms / 1e6, 1)},
         "speedup_vs_per_item_graph": round(graph_ms / ragged_ms, 2),
         "hbm_frac_one_pass_bytes": round(points * 16 / (ragged_ms / 1e3) / 1e9 / peak, 3),
+        "hbm_frac_min_pass_bytes": round(min_bytes / (ragged_ms / 1e3) / 1e9 / peak, 3),
     }
     del graph
     plan.destroy()

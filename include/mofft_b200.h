@@ -117,16 +117,23 @@ double mofft_schedule_model_seconds(int precision_bits, size_t length, size_t ba
                                     const int *kernels, size_t pass_count);
 
 /* Ragged batches (no counterpart in the reference): many FP32 transforms of
- * different lengths, batch sizes and directions executed by ONE persistent
- * kernel launch over a work-descriptor queue, replayed from a CUDA graph.
- * Items hold device buffers (input == output runs in place).  Supported
- * lengths: 2^6 .. 2^13 and 3*2^5 .. 3*2^11 in one pass, and products of two
- * column lengths in {96, 128, 192, 256} (e.g. 2^14 .. 2^16, 3*2^12, 3*2^13)
- * in two passes; others give MOFFT_UNSUPPORTED_SIZE.
+ * different lengths, batch sizes and directions in one CUDA graph.  Items
+ * hold device buffers (input == output runs in place).  Items of the lengths
+ * one persistent kernel runs in one pass (2^6 .. 2^13, 3*2^5 .. 3*2^11) are
+ * tiles of its work-descriptor queue (one launch for all of them); the other
+ * items are grouped by (length, direction), and each group runs its tuned
+ * schedule (compiled wisdom, else the model) once over all its transforms
+ * through pointer tables, one launch per pass.  A group whose schedule does
+ * not run through tables (more than two passes, a runtime-stage kernel)
+ * joins the persistent queue as two-pass tiles, which take products of two
+ * column lengths in {96, 128, 192, 256}; other lengths give
+ * MOFFT_UNSUPPORTED_SIZE.  mofft_ragged_plan_create_single_launch_f32 puts
+ * every item into the persistent queue (one launch in all).
  * mofft_ragged_execute enqueues the whole batch on `stream` (a
  * cudaStream_t); mofft_ragged_status (blocking) reports whether the last
- * execution completed every tile.  mofft_ragged_execute_per_item runs the
- * same items as one ordinary batched plan each (the comparison point). */
+ * execution completed every tile and every bounded wait of the groups'
+ * kernels.  mofft_ragged_execute_per_item runs the same items as one
+ * ordinary batched plan each (the comparison point). */
 typedef struct mofft_ragged_plan mofft_ragged_plan;
 typedef struct {
   size_t length;
@@ -138,16 +145,20 @@ typedef struct {
 mofft_status mofft_ragged_plan_create_f32(mofft_ragged_plan **plan,
                                           const mofft_ragged_item *items,
                                           size_t count);
+mofft_status mofft_ragged_plan_create_single_launch_f32(mofft_ragged_plan **plan,
+                                                        const mofft_ragged_item *items,
+                                                        size_t count);
 mofft_status mofft_ragged_execute(mofft_ragged_plan *plan, void *stream);
 mofft_status mofft_ragged_execute_per_item(mofft_ragged_plan *plan,
                                            void *stream);
 mofft_status mofft_ragged_status(mofft_ragged_plan *plan);
-/* Failure check: runs the plan's queue once on `stream` with every
- * second-pass dependency made unsatisfiable, so each second-pass tile gives
- * up after its bounded wait (about a second per tile and CTA) and skips its
- * work; mofft_ragged_status then reports MOFFT_INTERNAL_ERROR and the next
- * mofft_ragged_execute runs normally.  Plans without two-pass items have no
- * waits and report success.  For tests of the timeout path. */
+/* Failure check: runs the plan's persistent queue once on `stream` with
+ * every second-pass dependency made unsatisfiable, so each second-pass tile
+ * gives up after its bounded wait (about a second per tile and CTA) and skips
+ * its work; mofft_ragged_status then reports MOFFT_INTERNAL_ERROR and the
+ * next mofft_ragged_execute runs normally.  Plans without two-pass tiles
+ * (every plan whose long items all run as tuned groups) have no waits and
+ * report success.  For tests of the timeout path. */
 mofft_status mofft_ragged_check_lost_dependency(mofft_ragged_plan *plan,
                                                 void *stream);
 mofft_status mofft_ragged_plan_info(const mofft_ragged_plan *plan,

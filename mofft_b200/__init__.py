@@ -199,6 +199,8 @@ _PLAIN = [
     ("mofft_plan_check_f32", _I, [_P]),
     ("mofft_plan_check_lost_copy_f32", _I, [_P, _P, _P]),
     ("mofft_ragged_plan_create_f32", _I, [ctypes.POINTER(_P), ctypes.POINTER(RaggedItem), _SZ]),
+    ("mofft_ragged_plan_create_single_launch_f32", _I,
+     [ctypes.POINTER(_P), ctypes.POINTER(RaggedItem), _SZ]),
     ("mofft_ragged_execute", _I, [_P, _P]),
     ("mofft_ragged_execute_per_item", _I, [_P, _P]),
     ("mofft_ragged_status", _I, [_P]),
@@ -444,12 +446,15 @@ class Plan:
 
 
 class RaggedPlan:
-    """Many FP32 transforms of different lengths in one persistent launch.
+    """Many FP32 transforms of different lengths in one CUDA graph: the
+    one-pass lengths as tiles of one persistent launch, the longer ones as
+    tuned groups per (length, direction).  `single_launch` puts every item
+    into the persistent launch.
 
     `items` is a list of (input_tensor, output_tensor, direction) with
     complex64 CUDA tensors of shape (batch, n); input is output for in place."""
 
-    def __init__(self, items):
+    def __init__(self, items, single_launch: bool = False):
         self._lib = load()
         arr = (RaggedItem * len(items))()
         self._keep = []
@@ -458,8 +463,9 @@ class RaggedPlan:
             arr[k] = RaggedItem(n, x.numel() // n, direction, x.data_ptr(), y.data_ptr())
             self._keep.append((x, y))
         h = ctypes.c_void_p()
-        check(self._lib.mofft_ragged_plan_create_f32(ctypes.byref(h), arr, len(items)),
-              "ragged plan")
+        create = (self._lib.mofft_ragged_plan_create_single_launch_f32 if single_launch
+                  else self._lib.mofft_ragged_plan_create_f32)
+        check(create(ctypes.byref(h), arr, len(items)), "ragged plan")
         self._h = h
 
     def execute(self, stream: Optional[int] = None) -> None:

@@ -906,6 +906,18 @@ mofft_status mofft_core_create(mofft_core **out, int precision_bits,
                                  direction, placement, chain, chain_count, NULL);
 }
 
+mofft_status mofft_core_create_pretuned(mofft_core **out, int precision_bits, size_t length,
+                                        size_t batch, size_t distance,
+                                        mofft_direction direction, mofft_placement placement) {
+  int chain[MOFFT_MAX_STAGES];
+  int preferred[MOFFT_MAX_PASSES];
+  const int tuned = mofft_wisdom_lookup(length, precision_bits, chain, MOFFT_MAX_STAGES,
+                                        preferred);
+  return mofft_core_create_tuned(out, precision_bits, length, batch, distance, direction,
+                                 placement, tuned > 0 ? chain : NULL, tuned,
+                                 tuned > 0 ? preferred : NULL);
+}
+
 mofft_status mofft_core_create_tuned(mofft_core **out, int precision_bits,
                                      size_t length, size_t batch,
                                      size_t distance, mofft_direction direction,
@@ -1233,14 +1245,14 @@ mofft_status mofft_schedule_preview(int precision_bits, size_t length,
   return MOFFT_SUCCESS;
 }
 
-/* Indirect batch: `batch` transforms, transform b read from in_table[b] and
- * written to out_table[b] (device arrays of device pointers).  Out-of-place
- * routing only (the second pass of a two-pass schedule runs in place on the
- * output); schedules with a generic pass or more than two passes are not
- * supported (MOFFT_UNSUPPORTED_SIZE). */
-mofft_status mofft_core_enqueue_indirect(const mofft_core *c, const void *const *in_table,
-                                         void *const *out_table, long long batch,
-                                         void *stream) {
+/* Pointer-table batch with one table pair per pass: pass p of transform b
+ * reads in_tables[p][b] and writes out_tables[p][b] (device arrays of device
+ * pointers), so a caller routes each transform through storage of its own
+ * between the passes.  Schedules of at most two passes of specialised kernels
+ * (MOFFT_UNSUPPORTED_SIZE otherwise).  Launches are counted by the caller. */
+mofft_status mofft_core_enqueue_tables(const mofft_core *c, const void *const *const *in_tables,
+                                       void *const *const *out_tables, long long batch,
+                                       void *stream) {
   const int P = c->sched.pass_count;
   if (P > 2 || batch <= 0) return MOFFT_UNSUPPORTED_SIZE;
   for (int p = 0; p < P; ++p)
@@ -1252,8 +1264,8 @@ mofft_status mofft_core_enqueue_indirect(const mofft_core *c, const void *const 
     const mofft_pass *ps = &c->sched.pass[p];
     mofft_pass_args a;
     memset(&a, 0, sizeof(a));
-    a.in_table = p == 0 ? in_table : (const void *const *)out_table;
-    a.out_table = out_table;
+    a.in_table = in_tables[p];
+    a.out_table = out_tables[p];
     a.tw = (const unsigned char *)c->d_twiddles + ps->tw_offset;
     a.tw_hi = (const unsigned char *)c->d_twiddles + ps->tw_hi_offset;
     a.tw_lo = (const unsigned char *)c->d_twiddles + ps->tw_lo_offset;
@@ -1272,11 +1284,25 @@ mofft_status mofft_core_enqueue_indirect(const mofft_core *c, const void *const 
     if (pass_has_status(ps))
       a.status = (int *)((unsigned char *)c->d_twiddles + ps->status_offset);
     const int err = mofft_cuda_launch_pass(ps->kernel, &a, stream);
-    atomic_fetch_add(&g_launches, 1);
     if (err != 0) {
       cudaGetLastError();
       return MOFFT_INTERNAL_ERROR;
     }
   }
   return MOFFT_SUCCESS;
+}
+
+/* Indirect batch: `batch` transforms, transform b read from in_table[b] and
+ * written to out_table[b] (device arrays of device pointers).  Out-of-place
+ * routing only (the second pass of a two-pass schedule runs in place on the
+ * output); schedules with a generic pass or more than two passes are not
+ * supported (MOFFT_UNSUPPORTED_SIZE). */
+mofft_status mofft_core_enqueue_indirect(const mofft_core *c, const void *const *in_table,
+                                         void *const *out_table, long long batch,
+                                         void *stream) {
+  const void *const *ins[2] = {in_table, (const void *const *)out_table};
+  void *const *outs[2] = {out_table, out_table};
+  const mofft_status st = mofft_core_enqueue_tables(c, ins, outs, batch, stream);
+  if (st == MOFFT_SUCCESS) atomic_fetch_add(&g_launches, (uint64_t)c->sched.pass_count);
+  return st;
 }

@@ -52,6 +52,14 @@ mofft_status mofft_core_enqueue(const mofft_core *c, const void *in, void *out,
 mofft_status mofft_core_enqueue_batch(const mofft_core *c, const void *in, void *out,
                                       size_t batch, size_t distance, void *stream);
 mofft_status mofft_core_execute(const mofft_core *c, const void *in, void *out);
+mofft_status mofft_core_enqueue_tables(const mofft_core *c, const void *const *const *in_tables,
+                                       void *const *const *out_tables, long long batch,
+                                       void *stream);
+/* A PRETUNED core: the compiled wisdom's schedule for (length, precision)
+ * where one exists, else the model's. */
+mofft_status mofft_core_create_pretuned(mofft_core **out, int precision_bits, size_t length,
+                                        size_t batch, size_t distance,
+                                        mofft_direction direction, mofft_placement placement);
 mofft_status mofft_core_enqueue_indirect(const mofft_core *c, const void *const *in_table,
                                          void *const *out_table, long long batch,
                                          void *stream);

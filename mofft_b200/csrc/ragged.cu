@@ -264,12 +264,25 @@ size_t round256(size_t x) { return (x + 255) & ~size_t(255); }
 
 }  // namespace
 
+// Items the persistent kernel does not run in one pass, grouped by (length,
+// direction): one tuned plan per group, run through pointer tables (one pair
+// per pass) so that a group takes one launch per pass whatever its items.
+struct RaggedGroup {
+  mofft_core *core = nullptr;
+  long long transforms = 0;
+  int passes = 0;
+  size_t table_off = 0;         // first pointer of this group's tables
+};
+
 struct mofft_ragged_plan {
   int device = 0;
   int item_count = 0;
   int tile_count = 0;
   int grid = 0;
   size_t smem = 0;
+  std::vector<RaggedGroup> groups;
+  void **d_ptr_tables = nullptr;  // every group's pointer tables
+  int graph_launches = 0;         // kernels one execution launches
   RItem *d_items = nullptr;
   RTile *d_tiles = nullptr;
   int *d_counters = nullptr;     // next, error, done[items]
@@ -287,9 +300,25 @@ static mofft_status ragged_fail(mofft_ragged_plan *p, mofft_status st) {
   return st;
 }
 
-extern "C" mofft_status mofft_ragged_plan_create_f32(mofft_ragged_plan **out,
-                                                     const mofft_ragged_item *items,
-                                                     size_t count) {
+// A tuned plan for one group, if its schedule runs through pointer tables
+// (at most two passes of specialised kernels).
+static mofft_core *group_core(long long n, mofft_direction direction, long long transforms) {
+  mofft_core *c = nullptr;
+  if (mofft_core_create_pretuned(&c, 32, (size_t)n, (size_t)transforms, (size_t)n, direction,
+                                 MOFFT_OUT_OF_PLACE) != MOFFT_SUCCESS)
+    return nullptr;
+  bool ok = c->sched.pass_count >= 1 && c->sched.pass_count <= 2;
+  for (int q = 0; ok && q < c->sched.pass_count; ++q)
+    ok = c->sched.pass[q].kind == MOFFT_KERNEL_ROWS || c->sched.pass[q].kind == MOFFT_KERNEL_COLS;
+  if (!ok) {
+    mofft_core_destroy(c);
+    return nullptr;
+  }
+  return c;
+}
+
+static mofft_status ragged_create(mofft_ragged_plan **out, const mofft_ragged_item *items,
+                                  size_t count, bool group_large) {
   if (!out) return MOFFT_INVALID_ARGUMENT;
   *out = nullptr;
   if (!items || count == 0 || count > (1u << 20)) return MOFFT_INVALID_ARGUMENT;
@@ -300,6 +329,41 @@ extern "C" mofft_status mofft_ragged_plan_create_f32(mofft_ragged_plan **out,
   p->items.assign(items, items + count);
   p->item_count = (int)count;
   p->work.assign(count, nullptr);
+  // --- items the persistent kernel does not run in one pass: tuned groups
+  std::vector<int> group_of(count, -1);
+  if (group_large) {
+    std::vector<std::pair<long long, int>> keys;   // (length, direction) per group
+    std::vector<long long> transforms;
+    for (size_t i = 0; i < count; ++i) {
+      const mofft_ragged_item &u = items[i];
+      if (!u.input || !u.output || u.batch == 0 || u.length < 2 ||
+          (u.direction != MOFFT_FORWARD && u.direction != MOFFT_BACKWARD) ||
+          rows_config_for((long long)u.length) >= 0)
+        continue;
+      const std::pair<long long, int> key((long long)u.length, (int)u.direction);
+      size_t g = 0;
+      while (g < keys.size() && keys[g] != key) ++g;
+      if (g == keys.size()) {
+        keys.push_back(key);
+        transforms.push_back(0);
+      }
+      transforms[g] += (long long)u.batch;
+      group_of[i] = (int)g;
+    }
+    std::vector<int> usable(keys.size(), -1);
+    for (size_t g = 0; g < keys.size(); ++g) {
+      mofft_core *c = group_core(keys[g].first, (mofft_direction)keys[g].second, transforms[g]);
+      if (!c) continue;   // these items stay in the persistent queue
+      RaggedGroup rg;
+      rg.core = c;
+      rg.transforms = transforms[g];
+      rg.passes = c->sched.pass_count;
+      usable[g] = (int)p->groups.size();
+      p->groups.push_back(rg);
+    }
+    for (size_t i = 0; i < count; ++i)
+      if (group_of[i] >= 0) group_of[i] = usable[group_of[i]];
+  }
   // --- shape every item and lay out its twiddle tables
   std::vector<RItem> host_items(count);
   std::vector<size_t> tw0_off(count), tw1_off(count), hi_off(count), lo_off(count);
@@ -315,6 +379,7 @@ extern "C" mofft_status mofft_ragged_plan_create_f32(mofft_ragged_plan **out,
     it.batch = (long long)u.batch;
     it.dist = (long long)u.length;
     it.sign = u.direction == MOFFT_BACKWARD ? -1.0f : 1.0f;
+    if (group_of[i] >= 0) continue;   // a tuned group runs it
     const int r = rows_config_for(it.n);
     if (r >= 0) {
       it.passes = 1;
@@ -358,6 +423,7 @@ extern "C" mofft_status mofft_ragged_plan_create_f32(mofft_ragged_plan **out,
   }
   std::vector<unsigned char> host_tw(tw_bytes + 256);
   for (size_t i = 0; i < count; ++i) {
+    if (group_of[i] >= 0) continue;
     const RItem &it = host_items[i];
     const ConfigInfo &c0 = config(it.cfg0);
     mofft_fill_stage_table(host_tw.data() + tw0_off[i], 32, c0.radices, c0.radix_count);
@@ -387,6 +453,7 @@ extern "C" mofft_status mofft_ragged_plan_create_f32(mofft_ragged_plan **out,
   // --- buffers, then the tile queue
   std::vector<RTile> first, second;
   for (size_t i = 0; i < count; ++i) {
+    if (group_of[i] >= 0) continue;
     RItem &it = host_items[i];
     it.in = static_cast<const float2 *>(items[i].input);
     it.out = static_cast<float2 *>(items[i].output);
@@ -425,12 +492,15 @@ extern "C" mofft_status mofft_ragged_plan_create_f32(mofft_ragged_plan **out,
   p->tile_count = (int)tiles.size();
   for (const ConfigInfo &c : kConfigs) p->smem = std::max(p->smem, c.smem);
   if (cudaMalloc(&p->d_items, count * sizeof(RItem)) != cudaSuccess ||
-      cudaMalloc(&p->d_tiles, tiles.size() * sizeof(RTile)) != cudaSuccess ||
+      cudaMalloc(&p->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(RTile)) !=
+          cudaSuccess ||
       cudaMalloc(&p->d_counters, (count + 2) * sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
     return ragged_fail(p, MOFFT_ALLOCATION_FAILURE);
   }
-  if (cudaMemcpyAsync(p->d_items, host_items.data(), count * sizeof(RItem),
+  if (cudaMemsetAsync(p->d_counters, 0, (count + 2) * sizeof(int), p->capture_stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(p->d_items, host_items.data(), count * sizeof(RItem),
                       cudaMemcpyHostToDevice, p->capture_stream) != cudaSuccess ||
       cudaMemcpyAsync(p->d_tiles, tiles.data(), tiles.size() * sizeof(RTile),
                       cudaMemcpyHostToDevice, p->capture_stream) != cudaSuccess ||
@@ -444,8 +514,70 @@ extern "C" mofft_status mofft_ragged_plan_create_f32(mofft_ragged_plan **out,
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ragged_kernel, kThreads, p->smem);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
   p->grid = std::max(1, std::min(per_sm * sms, p->tile_count));
+  // --- pointer tables of the tuned groups: per pass the inputs, then the
+  // outputs of its transforms; a two-pass transform goes through its output
+  // (out of place) or a workspace of its item (in place) between the passes
+  if (!p->groups.empty()) {
+    size_t total = 0;
+    for (RaggedGroup &g : p->groups) {
+      g.table_off = total;
+      total += (size_t)(2 * g.passes) * (size_t)g.transforms;
+    }
+    std::vector<void *> host(total, nullptr);
+    std::vector<long long> next(p->groups.size(), 0);
+    for (size_t i = 0; i < count; ++i) {
+      if (group_of[i] < 0) continue;
+      const RaggedGroup &g = p->groups[group_of[i]];
+      const mofft_ragged_item &u = items[i];
+      const long long n = (long long)u.length;
+      float2 *in = static_cast<float2 *>(const_cast<void *>(u.input));
+      float2 *outp = static_cast<float2 *>(u.output);
+      float2 *mid = outp;
+      if (g.passes == 2 && u.input == u.output) {
+        if (cudaMalloc(&p->work[i], (size_t)u.batch * (size_t)n * sizeof(float2)) !=
+            cudaSuccess) {
+          cudaGetLastError();
+          return ragged_fail(p, MOFFT_ALLOCATION_FAILURE);
+        }
+        mid = static_cast<float2 *>(p->work[i]);
+      }
+      const long long T = g.transforms;
+      void **tab = host.data() + g.table_off;
+      for (long long b = 0; b < (long long)u.batch; ++b) {
+        const long long t = next[group_of[i]]++;
+        tab[t] = in + b * n;
+        if (g.passes == 1) {
+          tab[T + t] = outp + b * n;
+        } else {
+          tab[T + t] = mid + b * n;
+          tab[2 * T + t] = mid + b * n;
+          tab[3 * T + t] = outp + b * n;
+        }
+      }
+    }
+    if (cudaMalloc(&p->d_ptr_tables, total * sizeof(void *)) != cudaSuccess ||
+        cudaMemcpyAsync(p->d_ptr_tables, host.data(), total * sizeof(void *),
+                        cudaMemcpyHostToDevice, p->capture_stream) != cudaSuccess ||
+        cudaStreamSynchronize(p->capture_stream) != cudaSuccess) {
+      cudaGetLastError();
+      return ragged_fail(p, MOFFT_ALLOCATION_FAILURE);
+    }
+  }
+  p->graph_launches = p->tile_count > 0 ? 1 : 0;
+  for (const RaggedGroup &g : p->groups) p->graph_launches += g.passes;
   *out = p;
   return MOFFT_SUCCESS;
+}
+
+extern "C" mofft_status mofft_ragged_plan_create_f32(mofft_ragged_plan **out,
+                                                     const mofft_ragged_item *items,
+                                                     size_t count) {
+  return ragged_create(out, items, count, true);
+}
+
+extern "C" mofft_status mofft_ragged_plan_create_single_launch_f32(
+    mofft_ragged_plan **out, const mofft_ragged_item *items, size_t count) {
+  return ragged_create(out, items, count, false);
 }
 
 static cudaError_t ragged_enqueue(mofft_ragged_plan *p, cudaStream_t s, int need_bias = 0) {
@@ -469,7 +601,19 @@ extern "C" mofft_status mofft_ragged_execute(mofft_ragged_plan *p, void *stream)
       cudaGetLastError();
       return MOFFT_INTERNAL_ERROR;
     }
-    const cudaError_t e = ragged_enqueue(p, p->capture_stream);
+    // the tuned groups, then the persistent queue
+    mofft_status gs = MOFFT_SUCCESS;
+    for (const RaggedGroup &rg : p->groups) {
+      void **tab = p->d_ptr_tables + rg.table_off;
+      const long long T = rg.transforms;
+      const void *const *ins[2] = {(const void *const *)tab, (const void *const *)(tab + 2 * T)};
+      void *const *outs[2] = {tab + T, tab + 3 * T};
+      gs = mofft_core_enqueue_tables(rg.core, ins, outs, T, p->capture_stream);
+      if (gs != MOFFT_SUCCESS) break;
+    }
+    const cudaError_t e = gs != MOFFT_SUCCESS ? cudaErrorUnknown
+                          : p->tile_count > 0  ? ragged_enqueue(p, p->capture_stream)
+                                               : cudaSuccess;
     cudaGraph_t g = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(p->capture_stream, &g);
     if (e != cudaSuccess || e2 != cudaSuccess || !g) {
@@ -489,7 +633,7 @@ extern "C" mofft_status mofft_ragged_execute(mofft_ragged_plan *p, void *stream)
     cudaGetLastError();
     return MOFFT_INTERNAL_ERROR;
   }
-  mofft_count_launches(1);
+  mofft_count_launches((uint64_t)p->graph_launches);
   return MOFFT_SUCCESS;
 }
 
@@ -500,6 +644,7 @@ extern "C" mofft_status mofft_ragged_execute(mofft_ragged_plan *p, void *stream)
 extern "C" mofft_status mofft_ragged_check_lost_dependency(mofft_ragged_plan *p,
                                                            void *stream) {
   if (!p) return MOFFT_INVALID_ARGUMENT;
+  if (p->tile_count == 0) return MOFFT_SUCCESS;
   if (ragged_enqueue(p, static_cast<cudaStream_t>(stream), 1 << 30) != cudaSuccess) {
     cudaGetLastError();
     return MOFFT_INTERNAL_ERROR;
@@ -515,6 +660,8 @@ extern "C" mofft_status mofft_ragged_status(mofft_ragged_plan *p) {
     cudaGetLastError();
     return MOFFT_INTERNAL_ERROR;
   }
+  for (const RaggedGroup &g : p->groups)
+    if (mofft_core_check_status(g.core) != MOFFT_SUCCESS) return MOFFT_INTERNAL_ERROR;
   return error ? MOFFT_INTERNAL_ERROR : MOFFT_SUCCESS;
 }
 
@@ -547,6 +694,9 @@ extern "C" void mofft_ragged_plan_destroy(mofft_ragged_plan *p) {
   if (p->graph) cudaGraphDestroy(p->graph);
   if (p->capture_stream) cudaStreamDestroy(p->capture_stream);
   for (mofft_plan_f32 *plan : p->item_plans) mofft_plan_destroy_f32(plan);
+  for (RaggedGroup &g : p->groups)
+    if (g.core) mofft_core_destroy(g.core);
+  if (p->d_ptr_tables) cudaFree(p->d_ptr_tables);
   for (void *w : p->work)
     if (w) cudaFree(w);
   if (p->d_items) cudaFree(p->d_items);

@@ -1,6 +1,8 @@
-"""Ragged batches in one persistent launch (work-descriptor queue, CUDA
-graph): every item against the oracle, bit-identical repeats, each item the
-same alone and in the mix, and the per-item comparison path."""
+"""Ragged batches in one CUDA graph (one-pass lengths as tiles of one
+persistent launch over a work-descriptor queue, longer ones as tuned groups
+through pointer tables; or every item in the persistent launch): every item
+against the oracle, bit-identical repeats, each item the same alone and in
+the mix, and the per-item comparison path."""
 from __future__ import annotations
 
 import numpy as np
@@ -31,16 +33,21 @@ def make_items(spec, seed=0, inplace=lambda k: False):
     return items
 
 
-def test_ragged_matches_oracle_and_repeats():
+@pytest.mark.parametrize("single_launch", [False, True])
+def test_ragged_matches_oracle_and_repeats(single_launch):
     import torch
     # every length of the workload at least once, small batches
     spec = [(n, 1 + (k % 5), -1 if k % 2 else 1) for k, n in enumerate(workloads.RAGGED_LENGTHS)]
     spec += workloads.ragged_spec(count=24, seed=5, max_batch=6)
     items = make_items(spec, inplace=lambda k: k % 3 == 1)
-    plan = m.RaggedPlan([(a, b, d) for a, b, d, _ in items])
+    plan = m.RaggedPlan([(a, b, d) for a, b, d, _ in items], single_launch=single_launch)
     tiles, grid = plan.info()
     assert tiles > 0 and grid > 0
+    before = m.launch_count()
     plan.execute()
+    launches = m.launch_count() - before
+    # one persistent launch, plus one launch per pass of every tuned group
+    assert launches == 1 if single_launch else launches > 1
     torch.cuda.synchronize()
     assert plan.status() == 0
     first = [b.clone() for _, b, _, _ in items]
@@ -112,7 +119,7 @@ def test_lost_dependency_times_out_and_context_stays_usable():
     import torch
     spec = [(16384, 1, -1), (256, 3, 1)]            # one two-pass item, one one-pass item
     items = make_items(spec, seed=11)
-    plan = m.RaggedPlan([(a, b, d) for a, b, d, _ in items])
+    plan = m.RaggedPlan([(a, b, d) for a, b, d, _ in items], single_launch=True)
     stream = torch.cuda.Stream()
     t0 = time.perf_counter()
     plan.check_lost_dependency(stream.cuda_stream)
@@ -122,6 +129,27 @@ def test_lost_dependency_times_out_and_context_stays_usable():
     assert waited < 30.0, waited                       # bounded: about a second per tile
     plan.execute(stream.cuda_stream)
     stream.synchronize()
+    assert plan.status() == m.Status.SUCCESS
+    for (src, out, d, x) in items:
+        n = x.shape[-1]
+        ref = oracle.fft_ld(x.cpu().numpy().astype(np.complex128), d)
+        assert rel_l2(out.cpu().numpy(), ref) <= fp32_tol(n), n
+    plan.destroy()
+
+
+def test_long_items_run_as_tuned_groups():
+    """Without two-pass tiles the persistent queue has no waits: the lost-
+    dependency run reports success, and the long items (in place and out of
+    place, both directions) still match the oracle."""
+    import torch
+    spec = [(65536, 3, -1), (65536, 2, 1), (24576, 2, -1), (256, 3, 1), (32768, 1, 1)]
+    items = make_items(spec, seed=4, inplace=lambda k: k in (1, 2))
+    plan = m.RaggedPlan([(a, b, d) for a, b, d, _ in items])
+    plan.check_lost_dependency()
+    torch.cuda.synchronize()
+    assert plan.status() == m.Status.SUCCESS
+    plan.execute()
+    torch.cuda.synchronize()
     assert plan.status() == m.Status.SUCCESS
     for (src, out, d, x) in items:
         n = x.shape[-1]
