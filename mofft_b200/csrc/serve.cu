@@ -117,9 +117,17 @@ mofft_core *plan_for(mofft_server *S, const mofft_request &r, mofft_status *st) 
     *st = MOFFT_SUCCESS;
     return it->second;
   }
+  // the tuned schedule (compiled wisdom) where one exists; the model's where
+  // the tuned one has more passes than a pointer-table group runs (two)
   mofft_core *c = nullptr;
-  *st = mofft_core_create(&c, r.precision_bits, r.length, 1, 0, r.direction,
-                          MOFFT_OUT_OF_PLACE, nullptr, 0);
+  *st = mofft_core_create_pretuned(&c, r.precision_bits, r.length, 1, 0, r.direction,
+                                   MOFFT_OUT_OF_PLACE);
+  if (*st == MOFFT_SUCCESS && c->sched.pass_count > 2) {
+    mofft_core_destroy(c);
+    c = nullptr;
+    *st = mofft_core_create(&c, r.precision_bits, r.length, 1, 0, r.direction,
+                            MOFFT_OUT_OF_PLACE, nullptr, 0);
+  }
   if (*st != MOFFT_SUCCESS) return nullptr;
   S->plans[key] = c;
   return c;
