@@ -64,6 +64,9 @@ def parse_args():
     p.add_argument("--out-of-place", action="store_true")
     p.add_argument("--form", choices=list(FORMS), default="fp32",
                    help="precision form of the FP32 plan (tensor-core forms: n=4096)")
+    p.add_argument("--kernel", action="append", default=None,
+                   help="run the main plan with these registry kernels, one per pass "
+                        "(by name; for profiling a given kernel)")
     p.add_argument("--sweep", action="store_true")
     p.add_argument("--serve", action="store_true",
                    help="serving stream: continuous batching vs serial per-request execution")
@@ -325,7 +328,8 @@ def workload_config(args) -> dict:
             "placement": "out-of-place" if args.out_of_place else "in-place",
             "inputs": f"uniform[-1,1) seeded; {size}-point working set of "
                       f"{held / 1e6:.0f} MB {relation}",
-            "parallelism": f"replicas x{args.gpus}", "form": args.form}
+            "parallelism": f"replicas x{args.gpus}", "form": args.form,
+            **({"kernels": list(args.kernel)} if args.kernel else {})}
 
 
 # --------------------------------------------------------------- GPU side
@@ -375,8 +379,12 @@ def run_gpu(args, world, rank, local):
     x = torch.view_as_complex(data)
     inplace = not args.out_of_place
     y = x if inplace else torch.empty_like(x)
+    explicit = None
+    if args.kernel:
+        index = {k["name"]: k["index"] for k in m.kernels()}
+        explicit = [index[name] for name in args.kernel]
     plan = m.Plan.create(n, args.direction, m.IN_PLACE if inplace else m.OUT_OF_PLACE,
-                         bits=bits, batch=batch)
+                         bits=bits, batch=batch, kernels=explicit)
     apply_form(plan, args)
     stream = torch.cuda.Stream()
     plan.set_stream(stream.cuda_stream)
