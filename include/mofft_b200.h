@@ -123,12 +123,13 @@ double mofft_schedule_model_seconds(int precision_bits, size_t length, size_t ba
  * tiles of its work-descriptor queue (one launch for all of them); the other
  * items are grouped by (length, direction), and each group runs its tuned
  * schedule (compiled wisdom, else the model) once over all its transforms
- * through pointer tables, one launch per pass.  A group whose schedule does
- * not run through tables (more than two passes, a runtime-stage kernel)
- * joins the persistent queue as two-pass tiles, which take products of two
- * column lengths in {96, 128, 192, 256}; other lengths give
- * MOFFT_UNSUPPORTED_SIZE.  mofft_ragged_plan_create_single_launch_f32 puts
- * every item into the persistent queue (one launch in all).
+ * through pointer tables, one launch per pass, on parallel graph branches
+ * next to the persistent launch.  A group whose schedule does not run through
+ * tables (more than two passes, a runtime-stage kernel) joins the persistent
+ * queue as two-pass tiles, which take products of two column lengths in
+ * {96, 128, 192, 256}; other lengths give MOFFT_UNSUPPORTED_SIZE.
+ * mofft_ragged_plan_create_single_launch_f32 puts every item into the
+ * persistent queue (one launch in all).
  * mofft_ragged_execute enqueues the whole batch on `stream` (a
  * cudaStream_t); mofft_ragged_status (blocking) reports whether the last
  * execution completed every tile and every bounded wait of the groups'

@@ -1,6 +1,19 @@
 // Ragged batches: many FP32 transforms of different lengths, batch sizes and
-// directions in ONE persistent kernel launch driven by a work-descriptor
-// queue (tiles), replayed from a CUDA graph.
+// directions in one CUDA graph.
+//
+// Persistent queue.  Items of the lengths one CTA tile runs in one pass
+// (2^6 .. 2^13, 3*2^5 .. 3*2^11) run in ONE persistent kernel launch driven
+// by a work-descriptor queue (tiles); in a single-launch plan every item
+// does.
+//
+// Groups.  The other items are grouped by (length, direction), and each
+// group runs that length's tuned schedule (compiled wisdom, else the model)
+// once over all the group's transforms: pointer tables, one pair per pass,
+// give every transform its own input, output and (for two-pass schedules in
+// place) workspace, so a group takes one launch per pass.  The graph runs the
+// groups on four parallel branches next to the persistent launch.  A group
+// whose tuned schedule cannot run from tables joins the persistent queue as
+// two-pass tiles.
 //
 // Tiles.  Every item (length n, batch, direction, buffers) is cut into
 // tiles of work for one 512-thread CTA: a single-pass tile computes
@@ -264,7 +277,7 @@ size_t round256(size_t x) { return (x + 255) & ~size_t(255); }
 
 }  // namespace
 
-// Items the persistent kernel does not run in one pass, grouped by (length,
+// Items the persistent queue does not run in one pass, grouped by (length,
 // direction): one tuned plan per group, run through pointer tables (one pair
 // per pass) so that a group takes one launch per pass whatever its items.
 struct RaggedGroup {
@@ -283,6 +296,13 @@ struct mofft_ragged_plan {
   std::vector<RaggedGroup> groups;
   void **d_ptr_tables = nullptr;  // every group's pointer tables
   int graph_launches = 0;         // kernels one execution launches
+  // the graph's parallel branches: groups spread over them (largest first,
+  // each to the branch with the fewest points so far) so that independent
+  // launches overlap on the device
+  static constexpr int kBranches = 4;
+  cudaStream_t branch[kBranches] = {};
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join[kBranches] = {};
   RItem *d_items = nullptr;
   RTile *d_tiles = nullptr;
   int *d_counters = nullptr;     // next, error, done[items]
@@ -329,7 +349,7 @@ static mofft_status ragged_create(mofft_ragged_plan **out, const mofft_ragged_it
   p->items.assign(items, items + count);
   p->item_count = (int)count;
   p->work.assign(count, nullptr);
-  // --- items the persistent kernel does not run in one pass: tuned groups
+  // --- tuned groups for the items without a one-pass tile configuration
   std::vector<int> group_of(count, -1);
   if (group_large) {
     std::vector<std::pair<long long, int>> keys;   // (length, direction) per group
@@ -436,7 +456,12 @@ static mofft_status ragged_create(mofft_ragged_plan **out, const mofft_ragged_it
       mofft_write_twiddles(host_tw.data() + lo_off[i], 32, (uint64_t)it.n, 0, 1, lo_n);
     }
   }
-  if (cudaStreamCreateWithFlags(&p->capture_stream, cudaStreamNonBlocking) != cudaSuccess) {
+  bool branches_ok = cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) == cudaSuccess;
+  for (int b = 0; b < mofft_ragged_plan::kBranches && branches_ok; ++b)
+    branches_ok = cudaStreamCreateWithFlags(&p->branch[b], cudaStreamNonBlocking) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&p->join[b], cudaEventDisableTiming) == cudaSuccess;
+  if (!branches_ok || cudaStreamCreateWithFlags(&p->capture_stream, cudaStreamNonBlocking) !=
+                          cudaSuccess) {
     cudaGetLastError();
     return ragged_fail(p, MOFFT_INTERNAL_ERROR);
   }
@@ -601,19 +626,40 @@ extern "C" mofft_status mofft_ragged_execute(mofft_ragged_plan *p, void *stream)
       cudaGetLastError();
       return MOFFT_INTERNAL_ERROR;
     }
-    // the tuned groups, then the persistent queue
+    // the persistent queue on the capture stream, the tuned groups on the
+    // branches forked from it, all joined before the graph ends
     mofft_status gs = MOFFT_SUCCESS;
-    for (const RaggedGroup &rg : p->groups) {
+    cudaError_t e = cudaEventRecord(p->fork, p->capture_stream);
+    for (int b = 0; b < mofft_ragged_plan::kBranches && e == cudaSuccess; ++b)
+      e = cudaStreamWaitEvent(p->branch[b], p->fork, 0);
+    if (e == cudaSuccess && p->tile_count > 0) e = ragged_enqueue(p, p->capture_stream);
+    std::vector<size_t> order(p->groups.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+    auto points = [&](size_t i) {
+      return (double)p->groups[i].transforms * (double)p->groups[i].core->length;
+    };
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t a, size_t b) { return points(a) > points(b); });
+    double load[mofft_ragged_plan::kBranches] = {0.0};
+    for (size_t i : order) {
+      if (e != cudaSuccess || gs != MOFFT_SUCCESS) break;
+      int b = 0;
+      for (int q = 1; q < mofft_ragged_plan::kBranches; ++q)
+        if (load[q] < load[b]) b = q;
+      load[b] += points(i);
+      const RaggedGroup &rg = p->groups[i];
       void **tab = p->d_ptr_tables + rg.table_off;
       const long long T = rg.transforms;
       const void *const *ins[2] = {(const void *const *)tab, (const void *const *)(tab + 2 * T)};
       void *const *outs[2] = {tab + T, tab + 3 * T};
-      gs = mofft_core_enqueue_tables(rg.core, ins, outs, T, p->capture_stream);
-      if (gs != MOFFT_SUCCESS) break;
+      gs = mofft_core_enqueue_tables(rg.core, ins, outs, T, p->branch[b]);
     }
-    const cudaError_t e = gs != MOFFT_SUCCESS ? cudaErrorUnknown
-                          : p->tile_count > 0  ? ragged_enqueue(p, p->capture_stream)
-                                               : cudaSuccess;
+    for (int b = 0; b < mofft_ragged_plan::kBranches; ++b) {
+      const cudaError_t r = cudaEventRecord(p->join[b], p->branch[b]);
+      const cudaError_t w = cudaStreamWaitEvent(p->capture_stream, p->join[b], 0);
+      if (e == cudaSuccess) e = r != cudaSuccess ? r : w;
+    }
+    if (gs != MOFFT_SUCCESS && e == cudaSuccess) e = cudaErrorUnknown;
     cudaGraph_t g = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(p->capture_stream, &g);
     if (e != cudaSuccess || e2 != cudaSuccess || !g) {
@@ -693,6 +739,11 @@ extern "C" void mofft_ragged_plan_destroy(mofft_ragged_plan *p) {
   if (p->exec) cudaGraphExecDestroy(p->exec);
   if (p->graph) cudaGraphDestroy(p->graph);
   if (p->capture_stream) cudaStreamDestroy(p->capture_stream);
+  for (int b = 0; b < mofft_ragged_plan::kBranches; ++b) {
+    if (p->branch[b]) cudaStreamDestroy(p->branch[b]);
+    if (p->join[b]) cudaEventDestroy(p->join[b]);
+  }
+  if (p->fork) cudaEventDestroy(p->fork);
   for (mofft_plan_f32 *plan : p->item_plans) mofft_plan_destroy_f32(plan);
   for (RaggedGroup &g : p->groups)
     if (g.core) mofft_core_destroy(g.core);
