@@ -52,8 +52,10 @@ multiply counts per radix, used by the host cost model).
 """
 from __future__ import annotations
 
+import json
 import math
 import sys
+from dataclasses import dataclass
 from decimal import Decimal, getcontext
 from fractions import Fraction
 from pathlib import Path
@@ -154,6 +156,7 @@ class Emitter:
         self.count = 0
         self.adds = 0
         self.muls = 0
+        self.instr = 0
 
     def tmp(self, expr: str, adds: int = 0, muls: int = 0) -> str:
         name = f"t{self.count}"
@@ -161,7 +164,37 @@ class Emitter:
         self.lines.append(f"  const T {name} = {expr};")
         self.adds += adds
         self.muls += muls
+        # a product feeding a sum fuses into one FMA: a temporary of m
+        # products and a sums costs max(a, m) instructions (a negation none)
+        self.instr += max(adds, muls) if muls else adds
         return name
+
+    def peak_live(self, outputs) -> int:
+        """Peak number of live temporaries in program order; the outputs stay
+        live to the end."""
+        import re
+        first, last = {}, {}
+        for i, line in enumerate(self.lines):
+            name, expr = line.split(" = ", 1)
+            name = name.split()[-1]
+            first[name] = i
+            last.setdefault(name, i)
+            for used in re.findall(r"\bt\d+\b", expr):
+                last[used] = i
+        end = len(self.lines)
+        for y in outputs:
+            for part in y:
+                for used in re.findall(r"\bt\d+\b", part):
+                    last[used] = end
+        delta = [0] * (end + 2)
+        for name, i in first.items():
+            delta[i] += 1
+            delta[last[name] + 1] -= 1
+        peak = live = 0
+        for d in delta:
+            live += d
+            peak = max(peak, live)
+        return peak
 
     # complex helpers: values are (re, im) tuples of temporaries/expressions
     def add(self, a, b):
@@ -410,9 +443,6 @@ class Emitter:
 FAMILIES = ("direct", "like_terms", "even_odd", "like_terms_even_odd", "vector_reuse",
             "like_terms_vector_reuse")
 FAMILY_ID = {name: i + 1 for i, name in enumerate(FAMILIES)}   # 0 = default codelet
-# codelet family per kernel bank (the default codelet where it is not defined)
-BANK_FAMILIES = {1: ("like_terms",), 2: ("like_terms_even_odd",),
-                 3: ("like_terms_vector_reuse",)}
 BANK_COUNT = 4
 
 
@@ -425,11 +455,122 @@ def family_defined(radix: int, fam: str) -> bool:
     return radix % 4 == 0
 
 
+# ---------------------------------------------------------------- portfolio
+# Candidates per radix (the counterpart of the reference compiler's candidate
+# enumeration, compiler/mofft_compiler/patterns.py:607-628): every
+# Cooley-Tukey split A x B of a composite radix (its sub-DFTs in their default
+# form), the conjugate-pair form of a prime radix, the radix-2 butterfly, and
+# every rewrite family defined for the radix (radices up to 16; larger ones
+# would not fit a thread's registers in matrix form).  Ranked by a
+# register-level cost model (model.py:293-323 ranks the reference's
+# candidates with its SME model):
+#   instructions  one per add, FMA-fused where a product feeds a sum;
+#   registers     the peak number of live temporaries in program order; each
+#                 value beyond REG_BUDGET costs SPILL_COST instructions (a
+#                 spill store and reload);
+#   cost          instructions + spill penalty; ties keep the default codelet
+#                 first, then the name order.
+# Banks (portfolio.py:31-35): bank 0 runs the default codelet of every radix
+# (the split of SPLIT, the form every tuned kernel was measured with); bank
+# B > 0 runs the best-ranked candidate carrying its family's rewrite
+# (BANK_REWRITE: like-terms, even-odd, vector-reuse; the combined forms carry
+# two), else the default codelet.
+
+REG_BUDGET = 64
+SPILL_COST = 2
+BANK_REWRITE = {1: "like_terms", 2: "even_odd", 3: "vector_reuse"}
+
+
+@dataclass(frozen=True)
+class Candidate:
+    radix: int
+    name: str            # "split_AxB", "prime", "radix2" or a family name
+    family: str | None   # the rewrite family, None for the default forms
+    adds: int
+    muls: int
+    instr: int
+    live: int
+    cost: int
+    default: bool        # the codelet bank 0 runs
+
+
+def _default_name(radix: int) -> str:
+    if radix == 2:
+        return "radix2"
+    if radix in SPLIT:
+        a, b = SPLIT[radix]
+        return f"split_{a}x{b}"
+    return "prime"
+
+
+def _measure(radix: int, name: str, family: str | None) -> Candidate:
+    em = Emitter()
+    loaded = [(em.tmp(f"re[{j}]"), em.tmp(f"im[{j}]")) for j in range(radix)]
+    if family is not None:
+        ys = em.family(loaded, family)
+    elif name.startswith("split_"):
+        a, b = (int(v) for v in name[len("split_"):].split("x"))
+        ys = em._cooley_tukey(loaded, a, b)
+    else:
+        ys = em.dft(loaded)
+    live = em.peak_live(ys)
+    cost = em.instr + SPILL_COST * max(0, live - REG_BUDGET)
+    return Candidate(radix, name, family, em.adds, em.muls, em.instr, live, cost,
+                     family is None and name == _default_name(radix))
+
+
+def candidates(radix: int) -> list[Candidate]:
+    """Every candidate codelet of a radix."""
+    names: list[tuple[str, str | None]] = []
+    if radix == 2:
+        names.append(("radix2", None))
+    elif any(radix % a == 0 for a in range(2, radix)):
+        for a in range(2, radix):
+            if radix % a == 0:
+                names.append((f"split_{a}x{radix // a}", None))
+    else:
+        names.append(("prime", None))
+    if radix <= 16:
+        names += [(fam, fam) for fam in FAMILIES if family_defined(radix, fam)]
+    return [_measure(radix, n, f) for n, f in names]
+
+
+def ranked(radix: int) -> list[Candidate]:
+    """Candidates of a radix, best first."""
+    return sorted(candidates(radix), key=lambda c: (c.cost, not c.default, c.name))
+
+
+def bank_candidate(radix: int, bank: int) -> Candidate:
+    """The codelet kernel bank `bank` runs for `radix`."""
+    order = ranked(radix)
+    if bank == 0:
+        return next(c for c in order if c.default)
+    rewrite = BANK_REWRITE[bank]
+    default = next(c for c in order if c.default)
+    return next((c for c in order if c.family and rewrite in c.family), default)
+
+
 def bank_family(radix: int, bank: int) -> str | None:
-    for fam in BANK_FAMILIES.get(bank, ()):
-        if family_defined(radix, fam):
-            return fam
-    return None
+    """Rewrite family of bank `bank`'s codelet for `radix`; None where the
+    bank runs the default codelet."""
+    if bank == 0 or radix > 16:
+        return None
+    c = bank_candidate(radix, bank)
+    return None if c.default else c.family
+
+
+def portfolio_report() -> dict:
+    """Every radix's ranked candidates and each bank's choice (JSON)."""
+    out = {"reg_budget": REG_BUDGET, "spill_cost": SPILL_COST, "radices": {}}
+    for radix in RADICES:
+        out["radices"][str(radix)] = {
+            "ranked": [{"name": c.name, "adds": c.adds, "muls": c.muls, "instr": c.instr,
+                        "live": c.live, "cost": c.cost, "default": c.default}
+                       for c in ranked(radix)],
+            "banks": [bank_candidate(radix, b if radix <= 16 else 0).name
+                      for b in range(BANK_COUNT)],
+        }
+    return out
 
 
 def emit_family(radix: int, fam: str) -> str:
@@ -476,7 +617,8 @@ def generate() -> tuple[str, str]:
     for radix in RADICES:
         text, adds, muls = emit_radix(radix)
         parts.append(text)
-        costs.append((radix, adds, muls))
+        default = bank_candidate(radix, 0)
+        costs.append((radix, adds, muls, default.instr, default.live))
     dispatch = ["template <int R> struct Dft;"]
     for radix in RADICES:
         dispatch.append(
@@ -513,13 +655,16 @@ def generate() -> tuple[str, str]:
     parts.append("\n".join(fam_lines) + "\n")
     cost_lines = [
         "// Generated by mofft_b200/codegen/gen_codelets.py -- do not edit.",
-        "// Real additions / multiplications of one forward radix-R codelet.",
+        "// Real additions / multiplications of one forward radix-R codelet (the",
+        "// default form), its instructions with products fused into sums (FMA)",
+        "// and its peak live temporaries.",
         "#pragma once",
-        "typedef struct { int radix; int adds; int muls; } mofft_codelet_cost;",
+        "typedef struct { int radix; int adds; int muls; int instr; int live; } "
+        "mofft_codelet_cost;",
         "static const mofft_codelet_cost k_mofft_codelet_costs[] = {",
     ]
-    for radix, adds, muls in costs:
-        cost_lines.append(f"  {{{radix}, {adds}, {muls}}},")
+    for radix, adds, muls, instr, live in costs:
+        cost_lines.append(f"  {{{radix}, {adds}, {muls}, {instr}, {live}}},")
     cost_lines.append("};")
     cost_lines.append(f"#define MOFFT_CODELET_COST_COUNT {len(costs)}")
     return "\n".join(parts), "\n".join(cost_lines) + "\n"
@@ -529,7 +674,9 @@ def main(argv: list[str]) -> int:
     out_dir = Path(argv[1]) if len(argv) > 1 else Path(__file__).resolve().parents[1] / "csrc" / "generated"
     out_dir.mkdir(parents=True, exist_ok=True)
     cuh, costs = generate()
-    for name, text in (("codelets.cuh", cuh), ("codelet_costs.h", costs)):
+    report = json.dumps(portfolio_report(), indent=1) + "\n"
+    for name, text in (("codelets.cuh", cuh), ("codelet_costs.h", costs),
+                       ("codelet_portfolio.json", report)):
         path = out_dir / name
         if not path.exists() or path.read_text() != text:
             path.write_text(text)

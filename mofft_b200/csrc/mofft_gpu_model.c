@@ -47,14 +47,11 @@
 #define GM_ISSUE_EFF 0.7
 
 static double codelet_instr_per_point(int radix) {
+  /* the generator's count: one instruction per add, a product feeding a sum
+   * fused into one FMA */
   for (int i = 0; i < MOFFT_CODELET_COST_COUNT; ++i)
-    if (k_mofft_codelet_costs[i].radix == radix) {
-      const double adds = k_mofft_codelet_costs[i].adds;
-      const double muls = k_mofft_codelet_costs[i].muls;
-      /* a multiply feeding an add fuses into one FMA */
-      const double fused = muls < adds ? muls : adds;
-      return (adds + muls - fused) / radix;
-    }
+    if (k_mofft_codelet_costs[i].radix == radix)
+      return (double)k_mofft_codelet_costs[i].instr / radix;
   return 8.0;
 }
 

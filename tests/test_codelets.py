@@ -3,6 +3,7 @@ reference's codelet evaluator (golden vectors) -- the role of the reference's
 compiler/mofft_compiler/validate.py candidate harness."""
 from __future__ import annotations
 
+import json
 import subprocess
 from pathlib import Path
 
@@ -157,15 +158,49 @@ def test_rewrite_family_codelets_match_reference_evaluator(harness, golden_codel
 
 
 def test_bank_codelet_choice():
-    """Kernel banks follow the reference's portfolio families
-    (portfolio.py:31-35): 1 like-terms, 2 even-odd, 3 vector-reuse, the
-    default codelet where a bank's family is not defined for the radix."""
+    """Kernel banks are chosen the way the reference's portfolio chooses
+    them (portfolio.py:31-35 over model.py's ranking): every candidate of a
+    radix is ranked by the cost model; bank 0 runs the default codelet, bank
+    1 / 2 / 3 the best-ranked candidate carrying the like-terms / even-odd /
+    vector-reuse rewrite, the default codelet where no candidate carries it."""
     assert gen_codelets.BANK_COUNT == 4
+    for radix in RADICES:
+        order = gen_codelets.ranked(radix)
+        costs = [c.cost for c in order]
+        assert costs == sorted(costs), radix
+        assert sum(c.default for c in order) == 1, radix
+        assert gen_codelets.bank_candidate(radix, 0).default
+        names = {c.name for c in order}
+        if radix > 2 and radix not in (3, 5, 7, 11, 13):
+            # every Cooley-Tukey split is a candidate
+            assert all(f"split_{a}x{radix // a}" in names
+                       for a in range(2, radix) if radix % a == 0), radix
+        for bank, rewrite in gen_codelets.BANK_REWRITE.items():
+            chosen = gen_codelets.bank_candidate(radix, bank)
+            carrying = [c for c in order if c.family and rewrite in c.family]
+            assert chosen == (carrying[0] if carrying else gen_codelets.bank_candidate(radix, 0))
+            fam = gen_codelets.bank_family(radix, bank)
+            assert fam == (None if radix > 16 or chosen.default else chosen.family)
+    # instances of the rule
     assert gen_codelets.bank_family(5, 1) == "like_terms"
-    assert gen_codelets.bank_family(6, 2) == "like_terms_even_odd"
-    assert gen_codelets.bank_family(5, 2) is None
-    assert gen_codelets.bank_family(8, 3) == "like_terms_vector_reuse"
-    assert gen_codelets.bank_family(6, 3) is None
+    assert gen_codelets.bank_family(5, 2) is None          # odd radix: no even-odd form
+    assert gen_codelets.bank_family(6, 3) is None          # 6 % 4 != 0: no vector reuse
+    assert gen_codelets.bank_family(16, 3) == "like_terms_vector_reuse"
+    # the generated kernels run exactly these choices
+    text = (ROOT / "mofft_b200" / "csrc" / "generated" / "codelets.cuh").read_text()
+    for radix in (r for r in RADICES if r <= 16):
+        for bank in range(1, gen_codelets.BANK_COUNT):
+            fam = gen_codelets.bank_family(radix, bank)
+            spec = f"struct BankDft<{radix}, {bank}> : DftFamily<{radix}, "
+            if fam is None:
+                assert spec not in text, (radix, bank)
+            else:
+                want = spec + f"{gen_codelets.FAMILY_ID[fam]}>"
+                assert want in text, (radix, bank)
+    report = json.loads((ROOT / "mofft_b200" / "csrc" / "generated" /
+                         "codelet_portfolio.json").read_text())
+    assert report["radices"]["16"]["banks"][0] == "split_4x4"
+    assert report["radices"]["16"]["ranked"][0]["name"] == "split_4x4"
 
 
 def test_constants_correctly_rounded():
