@@ -470,11 +470,12 @@ def family_defined(radix: int, fam: str) -> bool:
 #                 spill store and reload);
 #   cost          instructions + spill penalty; ties keep the default codelet
 #                 first, then the name order.
-# Banks (portfolio.py:31-35): bank 0 runs the default codelet of every radix
-# (the split of SPLIT, the form every tuned kernel was measured with); bank
-# B > 0 runs the best-ranked candidate carrying its family's rewrite
-# (BANK_REWRITE: like-terms, even-odd, vector-reuse; the combined forms carry
-# two), else the default codelet.
+# Banks (portfolio.py:31-35): bank 0 -- every specialised kernel -- runs the
+# best-ranked candidate of every radix (ties keep the hand-chosen form: the
+# split of SPLIT, the conjugate-pair form of a prime); bank B > 0 runs the
+# best-ranked candidate carrying its family's rewrite (BANK_REWRITE:
+# like-terms, even-odd, vector-reuse; the combined forms carry two), else
+# bank 0's codelet.
 
 REG_BUDGET = 64
 SPILL_COST = 2
@@ -491,7 +492,7 @@ class Candidate:
     instr: int
     live: int
     cost: int
-    default: bool        # the codelet bank 0 runs
+    default: bool        # the hand-chosen form (SPLIT, prime, radix 2)
 
 
 def _default_name(radix: int) -> str:
@@ -540,14 +541,19 @@ def ranked(radix: int) -> list[Candidate]:
     return sorted(candidates(radix), key=lambda c: (c.cost, not c.default, c.name))
 
 
+def default_candidate(radix: int) -> Candidate:
+    """The codelet bank 0 (every specialised kernel) runs for `radix`: the
+    best-ranked candidate (ties keep the hand-chosen form)."""
+    return ranked(radix)[0]
+
+
 def bank_candidate(radix: int, bank: int) -> Candidate:
     """The codelet kernel bank `bank` runs for `radix`."""
-    order = ranked(radix)
+    default = default_candidate(radix)
     if bank == 0:
-        return next(c for c in order if c.default)
+        return default
     rewrite = BANK_REWRITE[bank]
-    default = next(c for c in order if c.default)
-    return next((c for c in order if c.family and rewrite in c.family), default)
+    return next((c for c in ranked(radix) if c.family and rewrite in c.family), default)
 
 
 def bank_family(radix: int, bank: int) -> str | None:
@@ -556,7 +562,7 @@ def bank_family(radix: int, bank: int) -> str | None:
     if bank == 0 or radix > 16:
         return None
     c = bank_candidate(radix, bank)
-    return None if c.default else c.family
+    return None if c == default_candidate(radix) else c.family
 
 
 def portfolio_report() -> dict:
@@ -588,13 +594,21 @@ def emit_family(radix: int, fam: str) -> str:
 
 
 def emit_radix(radix: int) -> tuple[str, int, int]:
+    """The default codelet of a radix: its best-ranked candidate."""
     em = Emitter()
     xs = []
     for j in range(radix):
         xs.append((f"re[{j}]", f"im[{j}]"))
     # Load inputs into named temporaries so writes to re/im cannot alias reads.
     loaded = [(em.tmp(x[0]), em.tmp(x[1])) for x in xs]
-    ys = em.dft(loaded)
+    best = default_candidate(radix)
+    if best.family is not None:
+        ys = em.family(loaded, best.family)
+    elif best.name.startswith("split_") and best.name != _default_name(radix):
+        a, b = (int(v) for v in best.name[len("split_"):].split("x"))
+        ys = em._cooley_tukey(loaded, a, b)
+    else:
+        ys = em.dft(loaded)
     body = list(em.lines)
     for k, (yr, yi) in enumerate(ys):
         body.append(f"  re[{k}] = {yr};")

@@ -9,7 +9,7 @@ static const mofft_codelet_cost k_mofft_codelet_costs[] = {
   {3, 12, 4, 14, 9},
   {4, 16, 0, 16, 11},
   {5, 32, 16, 36, 19},
-  {6, 40, 16, 48, 15},
+  {6, 40, 16, 40, 23},
   {7, 60, 36, 66, 27},
   {8, 52, 4, 56, 19},
   {9, 80, 40, 100, 21},
@@ -21,6 +21,6 @@ static const mofft_codelet_cost k_mofft_codelet_costs[] = {
   {15, 172, 100, 210, 39},
   {16, 144, 24, 160, 35},
   {32, 376, 88, 432, 67},
-  {64, 928, 248, 1088, 131},
+  {64, 920, 264, 1072, 131},
 };
 #define MOFFT_CODELET_COST_COUNT 17

@@ -160,16 +160,17 @@ def test_rewrite_family_codelets_match_reference_evaluator(harness, golden_codel
 def test_bank_codelet_choice():
     """Kernel banks are chosen the way the reference's portfolio chooses
     them (portfolio.py:31-35 over model.py's ranking): every candidate of a
-    radix is ranked by the cost model; bank 0 runs the default codelet, bank
-    1 / 2 / 3 the best-ranked candidate carrying the like-terms / even-odd /
-    vector-reuse rewrite, the default codelet where no candidate carries it."""
+    radix is ranked by the cost model; bank 0 runs the best-ranked candidate
+    (ties keep the hand-chosen form), bank 1 / 2 / 3 the best-ranked
+    candidate carrying the like-terms / even-odd / vector-reuse rewrite, the
+    bank-0 codelet where no candidate carries it."""
     assert gen_codelets.BANK_COUNT == 4
     for radix in RADICES:
         order = gen_codelets.ranked(radix)
         costs = [c.cost for c in order]
         assert costs == sorted(costs), radix
-        assert sum(c.default for c in order) == 1, radix
-        assert gen_codelets.bank_candidate(radix, 0).default
+        assert sum(c.default for c in order) == 1, radix      # one hand-chosen form
+        assert gen_codelets.bank_candidate(radix, 0) == order[0]
         names = {c.name for c in order}
         if radix > 2 and radix not in (3, 5, 7, 11, 13):
             # every Cooley-Tukey split is a candidate
@@ -180,7 +181,7 @@ def test_bank_codelet_choice():
             carrying = [c for c in order if c.family and rewrite in c.family]
             assert chosen == (carrying[0] if carrying else gen_codelets.bank_candidate(radix, 0))
             fam = gen_codelets.bank_family(radix, bank)
-            assert fam == (None if radix > 16 or chosen.default else chosen.family)
+            assert fam == (None if radix > 16 or chosen == order[0] else chosen.family)
     # instances of the rule
     assert gen_codelets.bank_family(5, 1) == "like_terms"
     assert gen_codelets.bank_family(5, 2) is None          # odd radix: no even-odd form
@@ -201,6 +202,10 @@ def test_bank_codelet_choice():
                          "codelet_portfolio.json").read_text())
     assert report["radices"]["16"]["banks"][0] == "split_4x4"
     assert report["radices"]["16"]["ranked"][0]["name"] == "split_4x4"
+    # where the model prefers another form, bank 0 runs it
+    assert report["radices"]["6"]["banks"][0] == "like_terms_even_odd"
+    assert report["radices"]["64"]["banks"][0] == "split_16x4"
+    assert "dft_fwd_6(" in text
 
 
 def test_constants_correctly_rounded():
