@@ -142,6 +142,41 @@ struct RowsLayout {
   __device__ __forceinline__ void super_twiddle(int, int, T (&)[R], T (&)[R]) const {}
 };
 
+// A line whose shared-memory exchanges move {re, im} pairs: one 8-byte
+// (FP32) / 16-byte (FP64) access per value instead of two.  One pad pair per
+// 16 pairs puts the stride-16 scatter of a radix-16 stage (Ns = 1) on
+// distinct bank pairs; the other gathers and scatters run 16 consecutive
+// pairs per half-warp.
+template <typename T>
+struct RowsPairLayout : RowsLayout<T> {
+  static constexpr bool kPairTag = true;
+  cplx_t<T>* sp;    // this line's shared pairs
+  __device__ __forceinline__ int paddr(int i) const { return i + (i >> 4); }
+  __device__ __forceinline__ void sget(int i, T& re, T& im) const {
+    const cplx_t<T> v = sp[paddr(i)];
+    re = v.x;
+    im = v.y;
+  }
+  __device__ __forceinline__ void sput(int i, T re, T im) const {
+    cplx_t<T> v;
+    v.x = re;
+    v.y = im;
+    sp[paddr(i)] = v;
+  }
+};
+
+// Pairs per line of a RowsPairLayout tile.
+__host__ __device__ constexpr int pair_line(int L) { return L + (L >> 4) + 1; }
+
+template <class Lay, class = void>
+struct IsPairLayout {
+  static constexpr bool value = false;
+};
+template <class Lay>
+struct IsPairLayout<Lay, decltype((void)Lay::kPairTag, void())> {
+  static constexpr bool value = true;
+};
+
 template <typename T, int C, int PITCH, bool TW>
 struct ColsLayout {
   T* sre;          // shared base of the tile (all C lines)
@@ -230,6 +265,7 @@ constexpr int kDerivedTw = 2;    // radix-16/32 twiddles from w, w^2, w^4, w^8 (
 constexpr int kSplitX = 4;       // exchanges move one component at a time
 constexpr int kTwoCtas = 8;      // registers capped for two resident CTAs per SM
 constexpr int kPrefetch = 16;    // persistent CTAs; the next line arrives by bulk copy
+constexpr int kPairX = 32;       // exchanges move {re, im} pairs (RowsPairLayout)
 
 // Twiddles of one radix-16 butterfly: v[r] *= w^r.  Loads the table entries
 // of w^1, w^2, w^4 and w^8 and forms the other powers with at most three
@@ -309,6 +345,8 @@ __device__ __forceinline__ void reg_stage(const Layout& lay, int t,
         const int idx = j + r * BF;
         if (SRC == kGlobal) {
           lay.gload(idx, vr[m][r], vi[m][r]);
+        } else if constexpr (IsPairLayout<Layout>::value) {
+          lay.sget(idx, vr[m][r], vi[m][r]);
         } else {
           vr[m][r] = lay.sre[lay.saddr(idx)];
           vi[m][r] = lay.sim[lay.saddr(idx)];
@@ -343,6 +381,8 @@ __device__ __forceinline__ void reg_stage(const Layout& lay, int t,
         const int idx = base + k * NS;
         if (DST == kGlobal) {
           lay.gstore(idx, vr[m][k], vi[m][k]);
+        } else if constexpr (IsPairLayout<Layout>::value) {
+          lay.sput(idx, vr[m][k], vi[m][k]);
         } else {
           lay.sre[lay.saddr(idx)] = vr[m][k];
           lay.sim[lay.saddr(idx)] = vi[m][k];
@@ -620,7 +660,13 @@ __device__ __forceinline__ void rows_body(const RowsArgs<T>& a, long long b0,
     }
     __syncthreads();
   }
-  if constexpr ((FLAGS & kSplitX) != 0) {
+  if constexpr ((FLAGS & kPairX) != 0) {
+    static_assert(!STAGED && (FLAGS & kSplitX) == 0, "pair exchanges: direct global I/O");
+    RowsPairLayout<T> lp;
+    static_cast<RowsLayout<T>&>(lp) = lay;
+    lp.sp = reinterpret_cast<cplx_t<T>*>(smem_raw) + line * pair_line(L);
+    StageRunner<T, L, TPL, 1, 0, false, false, true, DTW, Rs...>::run(lp, t, a.tw);
+  } else if constexpr ((FLAGS & kSplitX) != 0) {
     static_assert(!STAGED, "split exchanges run with direct global I/O");
     rows_body_split<T, L, TPL, TB, DTW, Rs...>(lay, sre + line * LINE, t, a.tw);
   } else {

@@ -50,6 +50,12 @@ const Entry *entries_rows_f32(int *count) {
       ROWSX(float, 8192, 512, 1, 16, 16, 16, 2),
       ROWSX(float, 16384, 512, 1, 16, 16, 16, 4),
       ROWSX(float, 16384, 1024, 1, 16, 16, 16, 4),
+      // exchanges move {re, im} pairs: one 8-byte shared access per value
+      ROWSDP(float, 1024, 64, 4, 16, 16, 4),
+      ROWSDP(float, 2048, 128, 2, 16, 16, 8),
+      ROWSDP(float, 4096, 256, 1, 16, 16, 16),
+      ROWSDP(float, 8192, 512, 1, 16, 16, 16, 2),
+      ROWSDP(float, 16384, 1024, 1, 16, 16, 16, 4),
       // persistent CTAs, next line bulk-copied while this one is transformed
       // (measured on 2^26 points against the kernels above: ahead only for
       // 16384, 0.55 against 0.51 of the HBM roofline; at 4096-12288 and for

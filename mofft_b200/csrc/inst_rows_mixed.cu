@@ -57,6 +57,15 @@ const Entry *entries_rows_mixed(int *count) {
       ROWSX(float, 6144, 384, 1, 6, 4, 16, 16),
       ROWSX(float, 10240, 640, 1, 5, 8, 16, 16),
       ROWSX(float, 12288, 768, 1, 3, 16, 16, 16),
+      // exchanges move {re, im} pairs
+      ROWSDP(float, 1536, 96, 2, 6, 16, 16),
+      ROWSDP(float, 3072, 192, 1, 12, 16, 16),
+      ROWSDP(float, 5120, 320, 1, 5, 4, 16, 16),
+      ROWSDP(float, 6144, 384, 1, 6, 4, 16, 16),
+      ROWSDP(float, 10240, 640, 1, 5, 8, 16, 16),
+      ROWSDP(float, 12288, 768, 1, 3, 16, 16, 16),
+      ROWSDP(double, 3072, 192, 1, 12, 16, 16),
+      ROWSDP(double, 6144, 384, 1, 6, 4, 16, 16),
       // derived radix-16 twiddles (5 table loads per butterfly instead of 15)
       ROWSD(float, 80, 5, 48, true, 5, 16),
       ROWSD(float, 96, 6, 32, true, 6, 16),
