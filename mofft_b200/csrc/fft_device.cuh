@@ -975,6 +975,67 @@ __device__ __forceinline__ void cols_body(const ColsArgs<T>& a, long long b,
   }
 }
 
+// Pair-exchange column tile: the C lines live in shared memory as {re, im}
+// pairs (element-major, ColsGeom's PITCH = C + 1 pairs per element row), so
+// each value crosses it as one 8- / 16-byte access; the odd pitch keeps the
+// first pass's contiguous output copy (stride PITCH) on distinct banks.
+template <typename T, int C, int PITCH, bool TW>
+struct ColsPairLayout : ColsLayout<T, C, PITCH, TW> {
+  static constexpr bool kPairTag = true;
+  cplx_t<T>* sp;
+  __device__ __forceinline__ int paddr(int i) const { return i * PITCH + this->c; }
+  __device__ __forceinline__ void sget(int i, T& re, T& im) const {
+    const cplx_t<T> v = sp[paddr(i)];
+    re = v.x;
+    im = v.y;
+  }
+  __device__ __forceinline__ void sput(int i, T re, T im) const {
+    cplx_t<T> v;
+    v.x = re;
+    v.y = im;
+    sp[paddr(i)] = v;
+  }
+};
+
+template <typename T, int L, int TPL, int C, int... Rs>
+__device__ __forceinline__ void cols_body_pair(const ColsArgs<T>& a, long long b,
+                                               long long j0, unsigned char* smem_raw) {
+  static_assert(StageProduct<L, Rs...>::value == L, "radices must multiply to L");
+  using G = ColsGeom<T, L, TPL, C>;
+  cplx_t<T>* sp = reinterpret_cast<cplx_t<T>*>(smem_raw);
+  const int t = threadIdx.x / C;
+  if (a.ns_outer == 1) {
+    ColsPairLayout<T, C, G::PITCH, false> lay;
+    cols_layout<T, L, TPL, C, false>(lay, a, b, j0, nullptr, nullptr);
+    lay.sp = sp;
+    StageRunner<T, L, TPL, 1, 0, false, true, true, true, Rs...>::run(lay, t, a.tw);
+    cplx_t<T>* dst = batch_out<T>(a.out, a.out_dist, a.out_table, b) + j0 * L;
+    if (lay.active) {
+      for (int q = threadIdx.x; q < C * L; q += G::THREADS) {
+        const int cc = q / L;
+        const int k = q - cc * L;
+        const cplx_t<T> v = sp[k * G::PITCH + cc];
+        st_global<T>(dst + q, v.x, v.y * a.sign_out);
+      }
+    }
+  } else {
+    ColsPairLayout<T, C, G::PITCH, true> lay;
+    cols_layout<T, L, TPL, C, true>(lay, a, b, j0, nullptr, nullptr);
+    lay.sp = sp;
+    StageRunner<T, L, TPL, 1, 0, false, false, true, true, Rs...>::run(lay, t, a.tw);
+  }
+}
+
+template <typename T, int L, int TPL, int C, int... Rs>
+__global__ void __launch_bounds__(TPL * C)
+cols_kernel_pair(const ColsArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const long long groups = (a.total / L) / C;
+  const long long b = blockIdx.x / groups;
+  const long long j0 = (blockIdx.x - b * groups) * C;
+  cols_body_pair<T, L, TPL, C, Rs...>(a, b, j0, smem_raw);
+}
+
 template <typename T, int L, int TPL, int C, int... Rs>
 __global__ void __launch_bounds__(TPL * C)
 cols_kernel(const ColsArgs<T> a) {

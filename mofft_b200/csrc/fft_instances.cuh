@@ -171,6 +171,43 @@ struct ColsInst {
   }
 };
 
+// Column pass whose exchanges move {re, im} pairs (cols_kernel_pair).
+template <typename T, int L, int TPL, int C, int... Rs>
+struct ColsPairInst {
+  using G = ColsGeom<T, L, TPL, C>;
+  static const void *func() {
+    return reinterpret_cast<const void *>(&cols_kernel_pair<T, L, TPL, C, Rs...>);
+  }
+  static cudaError_t launch(const mofft_pass_args *p, cudaStream_t s) {
+    if (p->total % L != 0 || (p->total / L) % C != 0) return cudaErrorInvalidValue;
+    if (p->ns_outer != 1 && p->ns_outer % C != 0) return cudaErrorInvalidValue;
+    const long long groups = (p->total / L) / C;
+    const long long grid = groups * p->batch;
+    if (grid <= 0) return cudaSuccess;
+    if (grid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    cols_kernel_pair<T, L, TPL, C, Rs...>
+        <<<(unsigned)grid, G::THREADS, G::SMEM, s>>>(cols_args<T>(p));
+    return cudaGetLastError();
+  }
+  static Entry entry(const char *name) {
+    Entry e{};
+    e.desc.name = name;
+    e.desc.precision_bits = sizeof(T) == 4 ? 32 : 64;
+    e.desc.kind = MOFFT_KERNEL_COLS;
+    e.desc.length = L;
+    e.desc.lines = C;
+    e.desc.threads = G::THREADS;
+    e.desc.staged = 0;
+    const int rs[] = {Rs...};
+    e.desc.radix_count = (int)sizeof...(Rs);
+    for (int i = 0; i < 8; ++i) e.desc.radices[i] = i < (int)sizeof...(Rs) ? rs[i] : 0;
+    e.desc.smem_bytes = G::SMEM;
+    e.launch = &launch;
+    e.func = &func;
+    return e;
+  }
+};
+
 template <typename T>
 size_t generic_smem(int L, int lines, int cols) {
   const size_t words = cols ? (size_t)L * (lines + 1) : (size_t)lines * spad_len<T>(L);
@@ -277,6 +314,8 @@ struct GenericInst {
       "rows_" #T "_" #L "_t" #TPL "_b1_sfalse_dxp2")
 #define COLS(T, L, TPL, C, ...) \
   ColsInst<T, L, TPL, C, __VA_ARGS__>::entry("cols_" #T "_" #L "_t" #TPL "_c" #C)
+#define COLSP(T, L, TPL, C, ...) \
+  ColsPairInst<T, L, TPL, C, __VA_ARGS__>::entry("cols_" #T "_" #L "_t" #TPL "_c" #C "_p")
 
 // Each instance file defines one of these.
 const Entry *entries_generic(int *count);

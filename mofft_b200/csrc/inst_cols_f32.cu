@@ -20,6 +20,12 @@ const Entry *entries_cols_f32(int *count) {
       COLS(float, 128, 8, 32, 16, 8),
       COLS(float, 512, 32, 8, 16, 16, 2),
       COLS(float, 1024, 64, 4, 16, 16, 4),
+      COLSP(float, 64, 4, 32, 16, 4),
+      COLSP(float, 128, 8, 16, 16, 8),
+      COLSP(float, 128, 8, 32, 16, 8),
+      COLSP(float, 256, 16, 16, 16, 16),
+      COLSP(float, 512, 32, 8, 16, 16, 2),
+      COLSP(float, 1024, 64, 8, 16, 16, 4),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;

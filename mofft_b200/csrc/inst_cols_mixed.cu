@@ -26,6 +26,16 @@ const Entry *entries_cols_mixed(int *count) {
       COLS(double, 320, 20, 8, 5, 4, 16),
       COLS(double, 640, 40, 8, 5, 8, 16),
       COLS(double, 1280, 80, 4, 5, 16, 16),
+      COLSP(float, 80, 5, 32, 5, 16),
+      COLSP(float, 160, 10, 16, 10, 16),
+      COLSP(float, 192, 12, 16, 12, 16),
+      COLSP(float, 1536, 96, 8, 6, 16, 16),
+      COLSP(double, 80, 5, 16, 5, 16),
+      COLSP(double, 96, 6, 16, 6, 16),
+      COLSP(double, 160, 10, 16, 10, 16),
+      COLSP(double, 192, 12, 16, 12, 16),
+      COLSP(double, 384, 24, 8, 6, 4, 16),
+      COLSP(double, 1536, 96, 4, 6, 16, 16),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;
