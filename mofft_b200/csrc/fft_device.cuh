@@ -588,6 +588,115 @@ __device__ __forceinline__ cplx_t<T>* batch_out(cplx_t<T>* base, long long dist,
   return table ? table[b] : base + b * dist;
 }
 
+// Pair-layout line pitch of a TB-line tile, in pairs: at least pair_line(L)
+// and, for TB > 1, congruent to the threads per line modulo one 128-byte row
+// of pairs, so that the lines a warp works on fall on distinct bank pairs.
+template <typename T>
+__host__ __device__ constexpr int pair_pitch(int L, int TPL, int TB) {
+  const int row = sizeof(T) == 4 ? 16 : 8;
+  int p = pair_line(L);
+  if (TB > 1)
+    while (p % row != TPL % row) ++p;
+  return p;
+}
+
+// ROWS tile whose line lives in shared memory as {re, im} pairs
+// (RowsPairLayout).  Staged tiles copy their lines between global and shared
+// memory as they are (interleaved complex), 16 bytes per access where the
+// tile is one dense aligned block, so the copies do no de-interleaving.
+template <typename T, int L, int TPL, int TB, bool STAGED, bool DTW, int... Rs>
+__device__ __forceinline__ void rows_body_pair(const RowsArgs<T>& a, long long b0,
+                                               unsigned char* smem_raw,
+                                               const RowsLayout<T>& lay, int line, int t) {
+  constexpr int PP = pair_pitch<T>(L, TPL, TB);
+  cplx_t<T>* sp = reinterpret_cast<cplx_t<T>*>(smem_raw);
+  RowsPairLayout<T> lp;
+  static_cast<RowsLayout<T>&>(lp) = lay;
+  lp.sp = sp + line * PP;
+  if constexpr (!STAGED) {
+    StageRunner<T, L, TPL, 1, 0, false, false, true, DTW, Rs...>::run(lp, t, a.tw);
+  } else {
+    constexpr int kThreadsTile = TPL * TB;
+    constexpr int kVecs = (int)(TB * L * sizeof(cplx_t<T>) / 16);
+    constexpr int kPer = kVecs / kThreadsTile;
+    constexpr int kPerVec = (int)(16 / sizeof(cplx_t<T>));
+    constexpr bool kVecOk = kVecs % kThreadsTile == 0 && kPer >= 1 && kPer <= 16 &&
+                            (TB * L * sizeof(cplx_t<T>)) % 16 == 0;
+    bool dense = false;
+    if constexpr (kVecOk) {
+      dense = a.in_table == nullptr && a.out_table == nullptr && a.in_dist == L &&
+              a.out_dist == L && b0 + TB <= a.batch &&
+              ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.out)) & 15) ==
+                  0;
+    }
+    const long long lines = (a.batch - b0) < TB ? (a.batch - b0) : TB;
+    if constexpr (kVecOk) {
+      if (dense) {
+        const uint4* src = reinterpret_cast<const uint4*>(a.in + b0 * L);
+        uint4 v[kPer];
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) v[k] = __ldcg(src + threadIdx.x + k * kThreadsTile);
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+          const cplx_t<T>* c = reinterpret_cast<const cplx_t<T>*>(&v[k]);
+#pragma unroll
+          for (int e = 0; e < kPerVec; ++e) {
+            const int q = (threadIdx.x + k * kThreadsTile) * kPerVec + e;
+            const int ln = q / L;
+            const int i = q - ln * L;
+            cplx_t<T> w = c[e];
+            w.y *= a.sign;
+            sp[ln * PP + lp.paddr(i)] = w;
+          }
+        }
+      }
+    }
+    if (!dense) {
+      for (int q = threadIdx.x; q < TB * L; q += kThreadsTile) {
+        const int ln = q / L;
+        const int i = q - ln * L;
+        if (ln < lines) {
+          cplx_t<T> w = ld_global<T>(batch_in<T>(a.in, a.in_dist, a.in_table, b0 + ln) + i);
+          w.y *= a.sign;
+          sp[ln * PP + lp.paddr(i)] = w;
+        }
+      }
+    }
+    __syncthreads();
+    StageRunner<T, L, TPL, 1, 0, true, true, true, DTW, Rs...>::run(lp, t, a.tw);
+    if constexpr (kVecOk) {
+      if (dense) {
+        uint4* dst = reinterpret_cast<uint4*>(a.out + b0 * L);
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+          uint4 v;
+          cplx_t<T>* c = reinterpret_cast<cplx_t<T>*>(&v);
+#pragma unroll
+          for (int e = 0; e < kPerVec; ++e) {
+            const int q = (threadIdx.x + k * kThreadsTile) * kPerVec + e;
+            const int ln = q / L;
+            const int i = q - ln * L;
+            c[e] = sp[ln * PP + lp.paddr(i)];
+            c[e].y *= a.sign;
+          }
+          dst[threadIdx.x + k * kThreadsTile] = v;
+        }
+      }
+    }
+    if (!dense) {
+      for (int q = threadIdx.x; q < TB * L; q += kThreadsTile) {
+        const int ln = q / L;
+        const int i = q - ln * L;
+        if (ln < lines) {
+          const cplx_t<T> w = sp[ln * PP + lp.paddr(i)];
+          st_global<T>(batch_out<T>(a.out, a.out_dist, a.out_table, b0 + ln) + i, w.x,
+                       w.y * a.sign);
+        }
+      }
+    }
+  }
+}
+
 // Body of one ROWS tile: transforms b0 .. b0+TB-1, run by threads
 // 0 .. TPL*TB-1 of the CTA (every thread of the CTA must call it).
 template <typename T, int L, int TPL, int TB, int FLAGS, int... Rs>
@@ -609,6 +718,11 @@ __device__ __forceinline__ void rows_body(const RowsArgs<T>& a, long long b0,
   lay.gin = lay.active ? batch_in<T>(a.in, a.in_dist, a.in_table, b) : a.in;
   lay.gout = lay.active ? batch_out<T>(a.out, a.out_dist, a.out_table, b) : a.out;
   lay.sign = a.sign;
+  if constexpr ((FLAGS & kPairX) != 0) {
+    static_assert((FLAGS & kSplitX) == 0, "pair and split exchanges exclude each other");
+    rows_body_pair<T, L, TPL, TB, STAGED, DTW, Rs...>(a, b0, smem_raw, lay, line, t);
+    return;
+  }
   // Dense full tile: the TB lines are one contiguous, 16-byte aligned block
   // of TB*L elements, copied with unrolled 16-byte vector accesses so that a
   // thread has all of its loads in flight at once.
@@ -660,13 +774,7 @@ __device__ __forceinline__ void rows_body(const RowsArgs<T>& a, long long b0,
     }
     __syncthreads();
   }
-  if constexpr ((FLAGS & kPairX) != 0) {
-    static_assert(!STAGED && (FLAGS & kSplitX) == 0, "pair exchanges: direct global I/O");
-    RowsPairLayout<T> lp;
-    static_cast<RowsLayout<T>&>(lp) = lay;
-    lp.sp = reinterpret_cast<cplx_t<T>*>(smem_raw) + line * pair_line(L);
-    StageRunner<T, L, TPL, 1, 0, false, false, true, DTW, Rs...>::run(lp, t, a.tw);
-  } else if constexpr ((FLAGS & kSplitX) != 0) {
+  if constexpr ((FLAGS & kSplitX) != 0) {
     static_assert(!STAGED, "split exchanges run with direct global I/O");
     rows_body_split<T, L, TPL, TB, DTW, Rs...>(lay, sre + line * LINE, t, a.tw);
   } else {

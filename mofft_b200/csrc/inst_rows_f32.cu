@@ -62,6 +62,14 @@ const Entry *entries_rows_f32(int *count) {
       // FP64 2048-8192 the same scheme measured 0-30 % slower, the lines
       // being bound by registers and exchanges rather than by load latency)
       ROWSP(float, 16384, 512, 32, 32, 16),
+      // staged tiles kept as {re, im} pairs (no de-interleaving copies)
+      ROWSSP(float, 16, 1, 256, 16),
+      ROWSSP(float, 32, 4, 64, 8, 4),
+      ROWSSP(float, 32, 2, 128, 16, 2),
+      ROWSSP(float, 64, 4, 64, 16, 4),
+      ROWSSP(float, 64, 8, 32, 8, 8),
+      ROWSSP(float, 128, 8, 32, 16, 8),
+      ROWSSP(float, 256, 16, 16, 16, 16),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;

@@ -34,6 +34,12 @@ const Entry *entries_rows_f64(int *count) {
       ROWSDP(double, 2048, 128, 2, 16, 16, 8),
       ROWSDP(double, 4096, 256, 1, 16, 16, 16),
       ROWSDP(double, 8192, 512, 1, 16, 16, 16, 2),
+      // staged tiles kept as {re, im} pairs
+      ROWSSP(double, 16, 1, 128, 16),
+      ROWSSP(double, 32, 4, 32, 8, 4),
+      ROWSSP(double, 64, 8, 16, 8, 8),
+      ROWSSP(double, 64, 4, 32, 16, 4),
+      ROWSSP(double, 128, 8, 16, 16, 8),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;
