@@ -30,6 +30,8 @@ const Entry *entries_rows_f64(int *count) {
       ROWSX(double, 4096, 256, 1, 16, 16, 16),
       ROWSX(double, 8192, 512, 1, 16, 16, 16, 2),
       // exchanges move {re, im} pairs: one 16-byte shared access per value
+      ROWSDP(double, 256, 16, 8, 16, 16),
+      ROWSDP(double, 512, 32, 4, 16, 16, 2),
       ROWSDP(double, 1024, 64, 2, 16, 16, 4),
       ROWSDP(double, 2048, 128, 2, 16, 16, 8),
       ROWSDP(double, 4096, 256, 1, 16, 16, 16),

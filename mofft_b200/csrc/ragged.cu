@@ -75,7 +75,8 @@ struct RTile {
 
 // Single-pass configurations: (id, L, TPL, staged, radices...) with
 // TB = 512 / TPL transforms per tile; radix-16 stages derive their twiddles
-// from four table entries, as the tuned standalone kernels do.
+// from four table entries and the tiles keep their lines as {re, im} pairs,
+// as the tuned standalone kernels do (the column tiles too).
 #define MOFFT_RAGGED_ROWS(X)                 \
   X(0, 64, 4, true, 16, 4)                  \
   X(1, 128, 8, true, 16, 8)                 \
@@ -115,7 +116,7 @@ constexpr int kArgCount = (int)sizeof...(R);
 
 #define MOFFT_ROWS_INFO(ID, L, TPL, ST, ...)                         \
   {ID, L, TPL, 0, kArgCount<__VA_ARGS__>, {__VA_ARGS__},             \
-   2ull * (kThreads / TPL) * rows_line<float>(L, TPL, kThreads / TPL) * sizeof(float)},
+   2ull * (kThreads / TPL) * pair_pitch<float>(L, TPL, kThreads / TPL) * sizeof(float)},
 #define MOFFT_COLS_INFO(ID, L, TPL, ...)                             \
   {ID, L, TPL, 1, kArgCount<__VA_ARGS__>, {__VA_ARGS__},             \
    ColsGeom<float, L, TPL, kColsLines>::SMEM},
@@ -177,14 +178,14 @@ __device__ __forceinline__ ColsArgs<float> cols_args_of(const RItem &it, int pas
   __device__ __noinline__ void tile_##ID(const RItem *__restrict__ itp, int pass,    \
                                          long long b, long long j0,                   \
                                          unsigned char *smem) {                       \
-    rows_body<float, L, TPL, kThreads / TPL, ((ST) ? kStaged : 0) | kDerivedTw,          \
+    rows_body<float, L, TPL, kThreads / TPL, ((ST) ? kStaged : 0) | kDerivedTw | kPairX, \
               __VA_ARGS__>(rows_args_of(*itp), b, smem);                               \
   }
 #define MOFFT_COLS_FN(ID, L, TPL, ...)                                              \
   __device__ __noinline__ void tile_##ID(const RItem *__restrict__ itp, int pass,    \
                                          long long b, long long j0,                   \
                                          unsigned char *smem) {                       \
-    cols_body<float, L, TPL, kColsLines, __VA_ARGS__>(cols_args_of(*itp, pass), b, j0, \
+    cols_body_pair<float, L, TPL, kColsLines, __VA_ARGS__>(cols_args_of(*itp, pass), b, j0, \
                                                       smem);                          \
   }
 MOFFT_RAGGED_ROWS(MOFFT_ROWS_FN)
