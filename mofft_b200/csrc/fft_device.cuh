@@ -147,11 +147,13 @@ struct RowsLayout {
 // 16 pairs puts the stride-16 scatter of a radix-16 stage (Ns = 1) on
 // distinct bank pairs; the other gathers and scatters run 16 consecutive
 // pairs per half-warp.
-template <typename T>
+// SH: one pad pair per 2^SH pairs (0: no padding, for lines whose
+// first-stage stride is odd, e.g. the radix-5 stage of 5*2^k lengths).
+template <typename T, int SH = 4>
 struct RowsPairLayout : RowsLayout<T> {
   static constexpr bool kPairTag = true;
   cplx_t<T>* sp;    // this line's shared pairs
-  __device__ __forceinline__ int paddr(int i) const { return i + (i >> 4); }
+  __device__ __forceinline__ int paddr(int i) const { return SH ? i + (i >> SH) : i; }
   __device__ __forceinline__ void sget(int i, T& re, T& im) const {
     const cplx_t<T> v = sp[paddr(i)];
     re = v.x;
@@ -166,7 +168,9 @@ struct RowsPairLayout : RowsLayout<T> {
 };
 
 // Pairs per line of a RowsPairLayout tile.
-__host__ __device__ constexpr int pair_line(int L) { return L + (L >> 4) + 1; }
+__host__ __device__ constexpr int pair_line(int L, int SH = 4) {
+  return SH ? L + (L >> SH) + 1 : L + 1;
+}
 
 template <class Lay, class = void>
 struct IsPairLayout {
@@ -266,6 +270,13 @@ constexpr int kSplitX = 4;       // exchanges move one component at a time
 constexpr int kTwoCtas = 8;      // registers capped for two resident CTAs per SM
 constexpr int kPrefetch = 16;    // persistent CTAs; the next line arrives by bulk copy
 constexpr int kPairX = 32;       // exchanges move {re, im} pairs (RowsPairLayout)
+constexpr int kPairPad32 = 64;   // with kPairX: one pad pair per 32 pairs
+constexpr int kPairPad0 = 128;   // with kPairX: no padding
+
+// Pad shift of a pair-exchange ROWS kernel's layout.
+__host__ __device__ constexpr int pair_shift(int flags) {
+  return (flags & kPairPad0) ? 0 : ((flags & kPairPad32) ? 5 : 4);
+}
 
 // Twiddles of one radix-16 butterfly: v[r] *= w^r.  Loads the table entries
 // of w^1, w^2, w^4 and w^8 and forms the other powers with at most three
@@ -592,9 +603,9 @@ __device__ __forceinline__ cplx_t<T>* batch_out(cplx_t<T>* base, long long dist,
 // and, for TB > 1, congruent to the threads per line modulo one 128-byte row
 // of pairs, so that the lines a warp works on fall on distinct bank pairs.
 template <typename T>
-__host__ __device__ constexpr int pair_pitch(int L, int TPL, int TB) {
+__host__ __device__ constexpr int pair_pitch(int L, int TPL, int TB, int SH = 4) {
   const int row = sizeof(T) == 4 ? 16 : 8;
-  int p = pair_line(L);
+  int p = pair_line(L, SH);
   if (TB > 1)
     while (p % row != TPL % row) ++p;
   return p;
@@ -604,13 +615,13 @@ __host__ __device__ constexpr int pair_pitch(int L, int TPL, int TB) {
 // (RowsPairLayout).  Staged tiles copy their lines between global and shared
 // memory as they are (interleaved complex), 16 bytes per access where the
 // tile is one dense aligned block, so the copies do no de-interleaving.
-template <typename T, int L, int TPL, int TB, bool STAGED, bool DTW, int... Rs>
+template <typename T, int L, int TPL, int TB, bool STAGED, bool DTW, int SH, int... Rs>
 __device__ __forceinline__ void rows_body_pair(const RowsArgs<T>& a, long long b0,
                                                unsigned char* smem_raw,
                                                const RowsLayout<T>& lay, int line, int t) {
-  constexpr int PP = pair_pitch<T>(L, TPL, TB);
+  constexpr int PP = pair_pitch<T>(L, TPL, TB, SH);
   cplx_t<T>* sp = reinterpret_cast<cplx_t<T>*>(smem_raw);
-  RowsPairLayout<T> lp;
+  RowsPairLayout<T, SH> lp;
   static_cast<RowsLayout<T>&>(lp) = lay;
   lp.sp = sp + line * PP;
   if constexpr (!STAGED) {
@@ -720,7 +731,8 @@ __device__ __forceinline__ void rows_body(const RowsArgs<T>& a, long long b0,
   lay.sign = a.sign;
   if constexpr ((FLAGS & kPairX) != 0) {
     static_assert((FLAGS & kSplitX) == 0, "pair and split exchanges exclude each other");
-    rows_body_pair<T, L, TPL, TB, STAGED, DTW, Rs...>(a, b0, smem_raw, lay, line, t);
+    rows_body_pair<T, L, TPL, TB, STAGED, DTW, pair_shift(FLAGS), Rs...>(a, b0, smem_raw, lay,
+                                                                         line, t);
     return;
   }
   // Dense full tile: the TB lines are one contiguous, 16-byte aligned block

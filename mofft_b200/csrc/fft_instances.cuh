@@ -65,7 +65,8 @@ struct RowsInst {
                 "prefetching kernels run one split-exchange line per CTA step");
   static constexpr size_t smem() {
     if constexpr (kPf) return prefetch_smem<T, L, TPL>();
-    if constexpr ((FLAGS & kPairX) != 0) return 2ull * TB * pair_pitch<T>(L, TPL, TB) * sizeof(T);
+    if constexpr ((FLAGS & kPairX) != 0)
+      return 2ull * TB * pair_pitch<T>(L, TPL, TB, pair_shift(FLAGS)) * sizeof(T);
     return ((FLAGS & kSplitX) ? 1ull : 2ull) * TB * rows_line<T>(L, TPL, TB) * sizeof(T);
   }
   static const void *func() {
@@ -297,6 +298,12 @@ struct GenericInst {
 #define ROWSDP(T, L, TPL, TB, ...) \
   RowsInst<T, L, TPL, TB, kDerivedTw | kPairX, __VA_ARGS__>::entry( \
       "rows_" #T "_" #L "_t" #TPL "_b" #TB "_sfalse_dp")
+#define ROWSDP0(T, L, TPL, TB, ...) \
+  RowsInst<T, L, TPL, TB, kDerivedTw | kPairX | kPairPad0, __VA_ARGS__>::entry( \
+      "rows_" #T "_" #L "_t" #TPL "_b" #TB "_sfalse_dp0")
+#define ROWSDP5(T, L, TPL, TB, ...) \
+  RowsInst<T, L, TPL, TB, kDerivedTw | kPairX | kPairPad32, __VA_ARGS__>::entry( \
+      "rows_" #T "_" #L "_t" #TPL "_b" #TB "_sfalse_dp5")
 #define ROWSSP(T, L, TPL, TB, ...) \
   RowsInst<T, L, TPL, TB, kStaged | kDerivedTw | kPairX, __VA_ARGS__>::entry( \
       "rows_" #T "_" #L "_t" #TPL "_b" #TB "_strue_dp")
