@@ -26,6 +26,8 @@ const Entry *entries_cols_f32(int *count) {
       COLSP(float, 256, 16, 16, 16, 16),
       COLSP(float, 512, 32, 8, 16, 16, 2),
       COLSP(float, 1024, 64, 8, 16, 16, 4),
+      COLSP(float, 2048, 128, 8, 16, 16, 8),
+      COLSP(float, 4096, 256, 4, 16, 16, 16),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;

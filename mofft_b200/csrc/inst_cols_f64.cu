@@ -20,6 +20,7 @@ const Entry *entries_cols_f64(int *count) {
       COLSP(double, 256, 16, 8, 16, 16),
       COLSP(double, 512, 32, 8, 16, 16, 2),
       COLSP(double, 1024, 64, 4, 16, 16, 4),
+      COLSP(double, 2048, 128, 4, 16, 16, 8),
   };
   *count = (int)(sizeof(e) / sizeof(e[0]));
   return e;
