@@ -53,6 +53,8 @@ const Entry *entries_rows_f32(int *count) {
       // exchanges move {re, im} pairs: one 8-byte shared access per value
       ROWSDP(float, 512, 32, 8, 16, 16, 2),
       ROWSDP(float, 1024, 64, 4, 16, 16, 4),
+      ROWSDP(float, 1024, 64, 2, 16, 16, 4),
+      ROWSDP(float, 2048, 128, 1, 16, 16, 8),
       ROWSDP(float, 2048, 128, 2, 16, 16, 8),
       ROWSDP(float, 4096, 256, 1, 16, 16, 16),
       ROWSDP(float, 8192, 512, 1, 16, 16, 16, 2),
